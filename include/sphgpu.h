@@ -1,0 +1,250 @@
+/*
+ * sphgpu.h — C ABI of the B200 (sm_100a) SPH per-step particle hot path.
+ *
+ * This is the drop-in boundary for the reference's per-step module surface
+ * (Guo-astro/sph-code-simulation):
+ *
+ *   Module::initialize / Module::calculation        include/module.hpp:10-14
+ *   BHTree::initialize / resize / make / set_kernel
+ *          / neighbor_search / tree_force           include/bhtree.hpp:76-81
+ *   PreInteraction::calculation (ssph)              src/pre_interaction.cpp:39-169
+ *   disph::PreInteraction::calculation              src/disph/d_pre_interaction.cpp:21-162
+ *   gsph::PreInteraction::calculation               src/gsph/g_pre_interaction.cpp:27-144
+ *   FluidForce::calculation (ssph)                  src/fluid_force.cpp:26-86
+ *   disph::FluidForce::calculation                  src/disph/d_fluid_force.cpp:26-86
+ *   gsph::FluidForce::calculation                   src/gsph/g_fluid_force.cpp:44-171
+ *   GravityForce::calculation                       src/gravity_force.cpp:52-89
+ *   TimeStep::calculation                           src/timestep.cpp:18-38
+ *   Solver::predict / correct / integrate           src/solver.cpp:966-1113
+ *   Solver::compute_total_energies                  src/solver.cpp:1149-1175
+ *
+ * Conventions
+ *   - Every entry point returns int: 0 = ok, >0 = recoverable (already
+ *     handled internally, e.g. a neighbour-list capacity that was grown and
+ *     the walk re-run), <0 = fatal.  The message of the last error is
+ *     available from sphgpu_last_error().  The C++ wrapper in
+ *     sph-code-simulation_b200/host/sphgpu.hpp turns fatal codes into
+ *     sph::SPHException, the way THROW_ERROR does (include/exception.hpp:9-14).
+ *   - One CUDA stream per context.  A context is not thread-safe.
+ *   - All device memory is owned by the context.  Host arrays passed in are
+ *     plain pointers in the caller's particle order (the reference's
+ *     std::vector<SPHParticle> index order); the device keeps particles in
+ *     octree (Morton) order and un-permutes on download.
+ *   - There is no CPU fallback: without a usable sm_100 device every compute
+ *     entry point fails with SPHGPU_ERR_CUDA.
+ */
+#ifndef SPHGPU_H
+#define SPHGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- enums: same order as sph::SPHType / KernelType / RiemannSolverType
+ *      (include/parameters.hpp:8-31) ---- */
+enum sphgpu_sph_type { SPHGPU_SSPH = 0, SPHGPU_DISPH = 1, SPHGPU_GSPH = 2 };
+enum sphgpu_kernel   { SPHGPU_CUBIC_SPLINE = 0, SPHGPU_WENDLAND = 1 };
+enum sphgpu_riemann  { SPHGPU_RIEMANN_HLL = 0, SPHGPU_RIEMANN_ITERATIVE = 1 };
+enum sphgpu_precision { SPHGPU_FP64 = 0, SPHGPU_MIXED = 1 };
+enum sphgpu_guess    { SPHGPU_GUESS_NONE = 0, SPHGPU_GUESS_MLP = 1 };
+
+/* return codes */
+enum sphgpu_status {
+    SPHGPU_OK = 0,
+    SPHGPU_RETRIED = 1,            /* capacity grown and the pass re-run */
+    SPHGPU_ERR_ARG = -1,           /* bad argument */
+    SPHGPU_ERR_CUDA = -2,          /* CUDA runtime error / no device */
+    SPHGPU_ERR_NEIGHBOR_OVERFLOW = -3, /* > neighbor_number*1000 neighbours (src/bhtree.cpp:129-135) */
+    SPHGPU_ERR_NODE_POOL = -4,     /* more nodes than 5*N+1 (src/bhtree.cpp:222-224) */
+    SPHGPU_ERR_STATE = -5,         /* call out of order (e.g. force before tree) */
+    SPHGPU_ERR_NO_MLP = -6         /* riemann_guess = MLP without weights */
+};
+
+/* Subset of sph::SPHParameters (include/parameters.hpp:33-91) that the hot
+ * path reads.  Key names follow the JSON keys of Solver::read_parameterfile
+ * (src/solver.cpp:311-438); sphgpu_default_params() fills the same defaults. */
+typedef struct sphgpu_params {
+    int32_t sph_type;              /* SPHType: ssph / disph / gsph          */
+    int32_t kernel;                /* "kernel": cubic_spline / wendland     */
+    int32_t neighbor_number;       /* "neighborNumber" (50)                 */
+    int32_t iterative_sml;         /* "iterativeSmoothingLength" (1)        */
+    double  gamma;                 /* "gamma" (5/3)                         */
+    double  cfl_sound;             /* "cflSound" (0.3)                      */
+    double  cfl_force;             /* "cflForce" (0.125)                    */
+    double  av_alpha;              /* "avAlpha" (1.0)                       */
+    int32_t use_balsara_switch;    /* "useBalsaraSwitch" (1)                */
+    int32_t use_time_dependent_av; /* "useTimeDependentAV" (0)              */
+    double  alpha_max;             /* "alphaMax" (2.0)                      */
+    double  alpha_min;             /* "alphaMin" (0.1)                      */
+    double  epsilon_av;            /* "epsilonAV" (0.2)                     */
+    int32_t use_ac;                /* "useArtificialConductivity" (0)       */
+    int32_t max_tree_level;        /* "maxTreeLevel" (20)                   */
+    double  alpha_ac;              /* "alphaAC" (1.0)                       */
+    int32_t leaf_particle_num;     /* "leafParticleNumber" (1)              */
+    int32_t periodic;              /* "periodic" (0)                        */
+    double  range_min[3];          /* "rangeMin"                            */
+    double  range_max[3];          /* "rangeMax"                            */
+    int32_t use_gravity;           /* "useGravity" (0)                      */
+    int32_t gsph_2nd_order;        /* "use2ndOrderGSPH" (1)                 */
+    double  g_constant;            /* "G" (1.0)                             */
+    double  theta;                 /* "theta" (0.5)                         */
+    int32_t riemann_solver;        /* "riemannSolver": hll / iterative      */
+    int32_t precision;             /* sphgpu_precision: FP64 drop-in / mixed */
+    int32_t riemann_guess;         /* sphgpu_guess: none / learned MLP      */
+    int32_t mlp_max_newton;        /* learned form: Newton iterations before
+                                      falling back to the plain solver (4)  */
+} sphgpu_params;
+
+/* Per-particle fields, in the order of sph::SPHParticle where it has them
+ * (include/particle.hpp:8-43), then the GSPH named arrays
+ * (src/solver.cpp:707-719). Used by upload/download. */
+enum sphgpu_field {
+    SPHGPU_F_POS_X = 0, SPHGPU_F_POS_Y, SPHGPU_F_POS_Z,
+    SPHGPU_F_VEL_X, SPHGPU_F_VEL_Y, SPHGPU_F_VEL_Z,
+    SPHGPU_F_VELP_X, SPHGPU_F_VELP_Y, SPHGPU_F_VELP_Z,
+    SPHGPU_F_ACC_X, SPHGPU_F_ACC_Y, SPHGPU_F_ACC_Z,
+    SPHGPU_F_MASS, SPHGPU_F_DENS, SPHGPU_F_PRES, SPHGPU_F_ENE, SPHGPU_F_ENE_P,
+    SPHGPU_F_DENE, SPHGPU_F_SML, SPHGPU_F_SOUND, SPHGPU_F_BALSARA,
+    SPHGPU_F_ALPHA, SPHGPU_F_GRADH, SPHGPU_F_PHI, SPHGPU_F_NEIGHBOR,
+    SPHGPU_F_GRAD_D_X, SPHGPU_F_GRAD_D_Y, SPHGPU_F_GRAD_D_Z,
+    SPHGPU_F_GRAD_P_X, SPHGPU_F_GRAD_P_Y, SPHGPU_F_GRAD_P_Z,
+    SPHGPU_F_GRAD_V0_X, SPHGPU_F_GRAD_V0_Y, SPHGPU_F_GRAD_V0_Z,
+    SPHGPU_F_GRAD_V1_X, SPHGPU_F_GRAD_V1_Y, SPHGPU_F_GRAD_V1_Z,
+    SPHGPU_F_GRAD_V2_X, SPHGPU_F_GRAD_V2_Y, SPHGPU_F_GRAD_V2_Z,
+    SPHGPU_NFIELDS
+};
+
+/* Device-side counters (no reference counterpart except the Newton
+ * non-convergence log line, src/pre_interaction.cpp:277-280). */
+typedef struct sphgpu_counters {
+    int64_t newton_nonconverged;   /* smoothing-length Newton fallbacks      */
+    int64_t riemann_solves;        /* iterative/learned Riemann solves       */
+    int64_t riemann_iterations;    /* Newton iterations summed over solves   */
+    int64_t riemann_fallbacks;     /* learned guess -> plain solver fallbacks */
+    int64_t gather_capacity;       /* current per-particle list capacity     */
+    int64_t max_gather;            /* largest gather list of the last search */
+    int64_t max_pair;              /* largest symmetric list                 */
+    int64_t node_count;            /* octree nodes of the last tree_make     */
+    int64_t retries;               /* neighbour walks re-run after growing   */
+} sphgpu_counters;
+
+/* Stage timers (ms, summed since the last reset; CUDA events on the
+ * context stream, recorded only when timing is enabled). */
+enum sphgpu_stage {
+    SPHGPU_T_TIMESTEP = 0, SPHGPU_T_PREDICT, SPHGPU_T_TREE, SPHGPU_T_GATHER_WALK,
+    SPHGPU_T_PRE, SPHGPU_T_SET_KERNEL, SPHGPU_T_PAIR_WALK, SPHGPU_T_FORCE,
+    SPHGPU_T_GRAVITY, SPHGPU_T_CORRECT, SPHGPU_NSTAGES
+};
+
+typedef struct sphgpu_ctx sphgpu_ctx;
+
+/* ---------------- parameters / lifetime ---------------- */
+void        sphgpu_default_params(sphgpu_params* p);
+int         sphgpu_create(const sphgpu_params* p, sphgpu_ctx** out);
+/* Simulation(param) + BHTree::initialize (src/simulation.cpp:13-33,
+   src/bhtree.cpp:13-41). */
+int         sphgpu_destroy(sphgpu_ctx* ctx);
+const char* sphgpu_last_error(const sphgpu_ctx* ctx);
+int         sphgpu_device_ok(void);  /* 1 if an sm_100 device is usable */
+
+/* ---------------- state transfer ---------------- */
+/* fields[k] may be NULL (field zero-filled).  Arrays are length n, in the
+   caller's particle order; the caller's index is the particle id.  Device
+   buffers are reused when n is unchanged; time, dt and h_per_v_sig persist
+   across uploads, and the next PreInteraction runs initial_smoothing unless
+   sphgpu_set_initial_smoothing(ctx, 0) is called. */
+int sphgpu_upload(sphgpu_ctx* ctx, int64_t n, const double* const* fields);
+/* fields[k] may be NULL (field skipped). */
+int sphgpu_download(sphgpu_ctx* ctx, double* const* fields);
+int64_t sphgpu_particle_num(const sphgpu_ctx* ctx);
+int sphgpu_get_time(const sphgpu_ctx* ctx, double* time, double* dt);
+int sphgpu_set_dt(sphgpu_ctx* ctx, double dt);
+int sphgpu_get_h_per_v_sig(const sphgpu_ctx* ctx, double* h_per_v_sig);
+
+/* ---------------- modules ---------------- */
+/* BHTree::make (src/bhtree.cpp:59-115): bbox, Morton keys replaying the
+   pos > center comparisons, radix sort, bottom-up node build, mass and
+   centre of mass.  Permutes the device particle arrays into tree order. */
+int sphgpu_tree_make(sphgpu_ctx* ctx);
+/* BHTree::set_kernel (src/bhtree.cpp:117-120,249-275). */
+int sphgpu_tree_set_kernel(sphgpu_ctx* ctx);
+/* Batched BHTree::neighbor_search (src/bhtree.cpp:122-144,277-316) for every
+   particle with radius sml (is_ij=0) or max(sml, node kernel_size)
+   (is_ij=1).  Writes a host CSR in caller order: offsets[n+1], ids[].
+   Pass ids=NULL to get the offsets (sizes) only.  Lists are in tree-walk
+   order (not distance-sorted). */
+int sphgpu_neighbor_search(sphgpu_ctx* ctx, int is_ij, int64_t* offsets,
+                           int32_t* ids, int64_t ids_capacity);
+/* Same, with the O(N^2) exhaustive predicate of exhaustive_search
+   (src/exhaustive_search.cpp:11-42). Debug/parity only. */
+int sphgpu_exhaustive_search(sphgpu_ctx* ctx, int is_ij, int64_t* offsets,
+                             int32_t* ids, int64_t ids_capacity);
+/* PreInteraction::calculation for params.sph_type, including
+   initial_smoothing on the first call and set_kernel at the end. */
+int sphgpu_pre_interaction(sphgpu_ctx* ctx);
+/* FluidForce::calculation for params.sph_type (overwrites acc and dene). */
+int sphgpu_fluid_force(sphgpu_ctx* ctx);
+/* GravityForce::calculation (adds to acc, sets phi). No-op without gravity. */
+int sphgpu_gravity_force(sphgpu_ctx* ctx);
+/* GravityForce::calculation under -DEXHAUSTIVE_SEARCH: direct summation
+   (src/gravity_force.cpp:70-84). Debug/parity only. */
+int sphgpu_gravity_direct(sphgpu_ctx* ctx);
+/* TimeStep::calculation: sets and returns dt. */
+int sphgpu_timestep(sphgpu_ctx* ctx, double* dt);
+/* Solver::predict / Solver::correct with the context dt. */
+int sphgpu_predict(sphgpu_ctx* ctx);
+int sphgpu_correct(sphgpu_ctx* ctx);
+/* Tail of Solver::initialize (src/solver.cpp:941-964): alpha = avAlpha,
+   balsara = 1, sound = sqrt(gamma (gamma-1) u), tree make, pre, force,
+   gravity. */
+int sphgpu_initialize(sphgpu_ctx* ctx);
+/* Solver::integrate (src/solver.cpp:966-978) followed by
+   Simulation::update_time. */
+int sphgpu_integrate(sphgpu_ctx* ctx);
+/* Solver::compute_total_energies (src/solver.cpp:1149-1175), plus total
+   momentum (mom[3]); FP64 device reductions. mom may be NULL. */
+int sphgpu_energies(sphgpu_ctx* ctx, double* kinetic, double* thermal,
+                    double* potential, double* mom);
+
+/* PreInteraction::m_first (src/pre_interaction.cpp:41-44): whether the next
+   PreInteraction call runs initial_smoothing first.  Set after upload; turn
+   it off to continue from a state whose density is already an SPH density
+   (e.g. a snapshot or another implementation's output). */
+int sphgpu_set_initial_smoothing(sphgpu_ctx* ctx, int on);
+/* Octree node table in depth-first preorder (children in index order), for
+   tree parity: ints[3k..] = level, is_leaf, particle count;
+   dbl[9k..] = center x,y,z, edge, mass, centre of mass x,y,z, kernel_size.
+   Returns the node count (call with NULL buffers to size), <0 on error. */
+int64_t sphgpu_tree_nodes(sphgpu_ctx* ctx, int32_t* ints, double* dbl, int64_t capacity);
+
+/* ---------------- diagnostics ---------------- */
+int sphgpu_get_counters(sphgpu_ctx* ctx, sphgpu_counters* out);
+int sphgpu_reset_counters(sphgpu_ctx* ctx);
+int sphgpu_enable_timing(sphgpu_ctx* ctx, int on);
+int sphgpu_get_stage_times(sphgpu_ctx* ctx, double* ms /* [SPHGPU_NSTAGES] */,
+                           int64_t* launches /* [SPHGPU_NSTAGES] or NULL */);
+int sphgpu_synchronize(sphgpu_ctx* ctx);
+/* CUDA-event timer on the context stream: elapsed device time between the
+   two calls (the stop call waits for the stream). */
+int sphgpu_timer_start(sphgpu_ctx* ctx);
+int sphgpu_timer_stop(sphgpu_ctx* ctx, double* ms);
+/* Kernels this context launched since timing was last enabled. */
+int64_t sphgpu_launch_count(const sphgpu_ctx* ctx);
+
+/* ---------------- learned Riemann guess (no reference counterpart) ------ */
+/* The MLP maps (log rho_R/rho_L, log p_R/p_L, (u_R-u_L)/c_L, c_R/c_L, gamma)
+   to log(p_star / p_L) through 3 hidden layers of 64 SiLU units. Weights are BF16
+   on the device, FP32 master copies in the trainer. */
+enum { SPHGPU_MLP_IN = 5, SPHGPU_MLP_HIDDEN = 64, SPHGPU_MLP_LAYERS = 3 };
+/* Number of FP32 parameters (weights + biases) of the MLP. */
+int64_t sphgpu_mlp_param_count(void);
+/* Load / read FP32 master parameters (length sphgpu_mlp_param_count()). */
+int sphgpu_mlp_set_params(sphgpu_ctx* ctx, const float* params);
+int sphgpu_mlp_get_params(sphgpu_ctx* ctx, float* params);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPHGPU_H */

@@ -1,0 +1,737 @@
+// capi.cu — the extern "C" boundary declared in include/sphgpu.h.
+//
+// Owns the context lifetime, device allocations, host <-> device transfer
+// (caller order <-> octree order) and the module sequencing of
+// Solver::initialize / Solver::integrate (src/solver.cpp:941-978).
+#include <algorithm>
+#include <cfloat>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "context.cuh"
+#include "mlp.cuh"
+
+namespace sphgpu {
+
+int fail(sphgpu_ctx* c, int code, const std::string& msg)
+{
+    if(c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(sphgpu_ctx* c, cudaError_t e, const char* where)
+{
+    std::string m = std::string("CUDA error in ") + where + ": " + cudaGetErrorString(e);
+    return fail(c, SPHGPU_ERR_CUDA, m);
+}
+
+static cudaEvent_t take_event(sphgpu_ctx* c)
+{
+    if(c->ev_pool.empty()) {
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    cudaEvent_t e = c->ev_pool.back();
+    c->ev_pool.pop_back();
+    return e;
+}
+
+void stage_begin(sphgpu_ctx* c, int stage)
+{
+    if(!c->timing) return;
+    c->open_ev[stage] = take_event(c);
+    cudaEventRecord(c->open_ev[stage], c->stream);
+}
+
+void stage_end(sphgpu_ctx* c, int stage, int launches)
+{
+    c->stage_launch[stage] += launches;
+    c->launches += launches;
+    if(!c->timing || !c->open_ev[stage]) return;
+    cudaEvent_t b = take_event(c);
+    cudaEventRecord(b, c->stream);
+    c->pending.push_back({stage, c->open_ev[stage], b});
+    c->open_ev[stage] = nullptr;
+}
+
+void stage_flush(sphgpu_ctx* c)
+{
+    for(auto& p : c->pending) {
+        float ms = 0.f;
+        if(cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) c->stage_ms[p.stage] += ms;
+        c->ev_pool.push_back(p.a);
+        c->ev_pool.push_back(p.b);
+    }
+    c->pending.clear();
+}
+
+int ensure_list_capacity(sphgpu_ctx* c, int which, int64_t cap)
+{
+    int*& list = which == 0 ? c->d_glist : c->d_plist;
+    int64_t& cur = which == 0 ? c->gcap : c->pcap;
+    if(cap <= cur && list) return SPHGPU_OK;
+    if(list) {
+        SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+        SPHGPU_CUDA(c, cudaFree(list));
+        list = nullptr;
+    }
+    const size_t bytes = sizeof(int) * (size_t)c->n * (size_t)cap;
+    SPHGPU_CUDA(c, cudaMalloc(&list, std::max<size_t>(bytes, 4)));
+    cur = cap;
+    return SPHGPU_OK;
+}
+
+namespace {
+
+void set_dev_params(sphgpu_ctx* c)
+{
+    const sphgpu_params& p = c->prm;
+    DevParams& d = c->dp;
+    d.sph_type = p.sph_type;
+    d.kernel = p.kernel;
+    d.nngb = p.neighbor_number;
+    d.iterative = p.iterative_sml;
+    d.gamma = p.gamma;
+    d.cfl_sound = p.cfl_sound;
+    d.cfl_force = p.cfl_force;
+    d.av_alpha = p.av_alpha;
+    d.balsara = p.use_balsara_switch;
+    d.td_av = p.use_time_dependent_av;
+    d.alpha_max = p.alpha_max;
+    d.alpha_min = p.alpha_min;
+    d.eps_av = p.epsilon_av;
+    d.use_ac = p.use_ac;
+    d.alpha_ac = p.alpha_ac;
+    d.max_level = p.max_tree_level;
+    d.leaf_num = p.leaf_particle_num;
+    d.periodic = p.periodic;
+    for(int k = 0; k < 3; ++k) {
+        d.lo[k] = p.range_min[k];
+        d.hi[k] = p.range_max[k];
+        d.range[k] = p.range_max[k] - p.range_min[k];
+    }
+    d.gravity = p.use_gravity;
+    d.G = p.g_constant;
+    d.theta = p.theta;
+    d.theta2 = p.theta * p.theta;
+    d.gsph2 = p.gsph_2nd_order;
+    d.riemann = p.riemann_solver;
+    d.precision = p.precision;
+    d.guess = p.riemann_guess;
+    d.mlp_max_newton = p.mlp_max_newton;
+    d.ratio = p.iterative_sml ? 1.2 : 1.0;
+}
+
+void free_all(sphgpu_ctx* c)
+{
+    for(void* p : c->state_allocs) cudaFree(p);
+    c->state_allocs.clear();
+    if(c->d_glist) cudaFree(c->d_glist);
+    if(c->d_plist) cudaFree(c->d_plist);
+    c->d_glist = c->d_plist = nullptr;
+    c->gcap = c->pcap = 0;
+}
+
+template <typename T>
+int dalloc(sphgpu_ctx* c, T*& p, size_t count)
+{
+    void* q = nullptr;
+    SPHGPU_CUDA(c, cudaMalloc(&q, std::max<size_t>(count * sizeof(T), 16)));
+    c->state_allocs.push_back(q);
+    p = static_cast<T*>(q);
+    return SPHGPU_OK;
+}
+
+int alloc_state(sphgpu_ctx* c, DevState& s, int n)
+{
+    s.n = n;
+    int rc = 0;
+    if((rc = dalloc(c, s.pos, n)) || (rc = dalloc(c, s.vel, n)) || (rc = dalloc(c, s.acc, n))
+       || (rc = dalloc(c, s.velp, n)) || (rc = dalloc(c, s.thermo, n)) || (rc = dalloc(c, s.visc, n))
+       || (rc = dalloc(c, s.grad, 4 * (size_t)n)) || (rc = dalloc(c, s.id, n)) || (rc = dalloc(c, s.nbr, n)))
+        return rc;
+    return SPHGPU_OK;
+}
+
+int alloc_all(sphgpu_ctx* c, int n)
+{
+    free_all(c);
+    c->n = n;
+    int rc = 0;
+    if((rc = alloc_state(c, c->s, n)) || (rc = alloc_state(c, c->alt, n))) return rc;
+    c->node_cap = 5 * n + 2;
+    const int nc = c->node_cap;
+    if((rc = dalloc(c, c->t.geo, nc)) || (rc = dalloc(c, c->t.mass, nc)) || (rc = dalloc(c, c->t.ksize, nc))
+       || (rc = dalloc(c, c->t.link, nc)) || (rc = dalloc(c, c->t.parent, nc)) || (rc = dalloc(c, c->t.nchild, nc))
+       || (rc = dalloc(c, c->t.counter, nc)) || (rc = dalloc(c, c->t.nnodes, 4)))
+        return rc;
+    if((rc = dalloc(c, c->d_root, 1)) || (rc = dalloc(c, c->d_bbox_part, 6 * 1024)) || (rc = dalloc(c, c->d_keys, n))
+       || (rc = dalloc(c, c->d_keys_alt, n)) || (rc = dalloc(c, c->d_vals, n)) || (rc = dalloc(c, c->d_vals_alt, n))
+       || (rc = dalloc(c, c->d_nstart, n)) || (rc = dalloc(c, c->d_base, n)) || (rc = dalloc(c, c->d_lvl, n))
+       || (rc = dalloc(c, c->d_leaf_of_start, n)) || (rc = dalloc(c, c->d_inv, n)) || (rc = dalloc(c, c->d_gcount, n))
+       || (rc = dalloc(c, c->d_pcount, n)) || (rc = dalloc(c, c->d_dt, 1)) || (rc = dalloc(c, c->d_hvs, 1))
+       || (rc = dalloc(c, c->d_red, 8 + 6 * 1024 + 64)) || (rc = dalloc(c, c->d_status, 1)))
+        return rc;
+    char* rs = nullptr;
+    if((rc = dalloc(c, rs, radix_scratch_bytes(n)))) return rc;
+    c->d_radix_scratch = rs;
+    char* ss = nullptr;
+    if((rc = dalloc(c, ss, scan_scratch_bytes(2LL * n + 2)))) return rc;
+    c->d_scan_scratch = ss;
+    scan_scratch_init(c->scan, ss, 2LL * n + 2);
+    const int64_t cap0 = ((int64_t)3 * c->prm.neighbor_number + 31) / 32 * 32;
+    if((rc = ensure_list_capacity(c, 0, cap0)) || (rc = ensure_list_capacity(c, 1, cap0))) return rc;
+    SPHGPU_CUDA(c, cudaMemsetAsync(c->d_status, 0, sizeof(DevStatus), c->stream));
+    const double zero = 0.0, big = DBL_MAX;
+    SPHGPU_CUDA(c, cudaMemcpyAsync(c->d_dt, &zero, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    SPHGPU_CUDA(c, cudaMemcpyAsync(c->d_hvs, &big, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    return SPHGPU_OK;
+}
+
+// field -> (array, component); component 4 = int array (nbr)
+struct FieldRef {
+    double4* arr;
+    int comp;
+};
+
+FieldRef field_ref(const DevState& s, int f)
+{
+    const size_t n = (size_t)s.n;
+    switch(f) {
+    case SPHGPU_F_POS_X: return {s.pos, 0};
+    case SPHGPU_F_POS_Y: return {s.pos, 1};
+    case SPHGPU_F_POS_Z: return {s.pos, 2};
+    case SPHGPU_F_MASS: return {s.pos, 3};
+    case SPHGPU_F_VEL_X: return {s.vel, 0};
+    case SPHGPU_F_VEL_Y: return {s.vel, 1};
+    case SPHGPU_F_VEL_Z: return {s.vel, 2};
+    case SPHGPU_F_SML: return {s.vel, 3};
+    case SPHGPU_F_ACC_X: return {s.acc, 0};
+    case SPHGPU_F_ACC_Y: return {s.acc, 1};
+    case SPHGPU_F_ACC_Z: return {s.acc, 2};
+    case SPHGPU_F_DENE: return {s.acc, 3};
+    case SPHGPU_F_VELP_X: return {s.velp, 0};
+    case SPHGPU_F_VELP_Y: return {s.velp, 1};
+    case SPHGPU_F_VELP_Z: return {s.velp, 2};
+    case SPHGPU_F_ENE_P: return {s.velp, 3};
+    case SPHGPU_F_DENS: return {s.thermo, 0};
+    case SPHGPU_F_PRES: return {s.thermo, 1};
+    case SPHGPU_F_ENE: return {s.thermo, 2};
+    case SPHGPU_F_SOUND: return {s.thermo, 3};
+    case SPHGPU_F_ALPHA: return {s.visc, 0};
+    case SPHGPU_F_BALSARA: return {s.visc, 1};
+    case SPHGPU_F_GRADH: return {s.visc, 2};
+    case SPHGPU_F_PHI: return {s.visc, 3};
+    case SPHGPU_F_NEIGHBOR: return {nullptr, 4};
+    default: {
+        const int g = f - SPHGPU_F_GRAD_D_X;
+        return {s.grad + (size_t)(g / 4) * n, g % 4};
+    }
+    }
+}
+
+__device__ __forceinline__ double& comp_of(double4& v, int c)
+{
+    return c == 0 ? v.x : (c == 1 ? v.y : (c == 2 ? v.z : v.w));
+}
+
+__global__ void k_put(double4* __restrict__ arr, int comp, const double* __restrict__ src, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < n) comp_of(arr[i], comp) = src ? src[i] : 0.0;
+}
+
+__global__ void k_put_nbr(int* __restrict__ nbr, const double* __restrict__ src, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < n) nbr[i] = src ? (int)src[i] : 0;
+}
+
+__global__ void k_get(const double4* __restrict__ arr, int comp, const int* __restrict__ id, double* __restrict__ dst,
+                      int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < n) {
+        double4 v = arr[i];
+        dst[id[i]] = comp_of(v, comp);
+    }
+}
+
+__global__ void k_get_nbr(const int* __restrict__ nbr, const int* __restrict__ id, double* __restrict__ dst, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < n) dst[id[i]] = (double)nbr[i];
+}
+
+// Solver::initialize (src/solver.cpp:941-953)
+__global__ void k_init_state(DevState S, int n, double alpha, double cs)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    double4 v = S.visc[i];
+    v.x = alpha;
+    v.y = 1.0;
+    S.visc[i] = v;
+    double4 t = S.thermo[i];
+    t.w = sqrt(cs * t.z);
+    S.thermo[i] = t;
+}
+
+__global__ void k_iota(int* __restrict__ id, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < n) id[i] = i;
+}
+
+int check_params(const sphgpu_params* p, std::string& why)
+{
+    if(p->sph_type < SPHGPU_SSPH || p->sph_type > SPHGPU_GSPH) return why = "SPH type must be ssph, disph or gsph", -1;
+    if(p->kernel != SPHGPU_CUBIC_SPLINE && p->kernel != SPHGPU_WENDLAND) return why = "kernel is unknown.", -1;
+    if(p->neighbor_number <= 0) return why = "neighborNumber must be positive", -1;
+    if(p->max_tree_level < 1 || p->max_tree_level > 21) return why = "maxTreeLevel must be in 1..21", -1;
+    if(p->leaf_particle_num < 1) return why = "leafParticleNumber must be >= 1", -1;
+    if(p->periodic) {
+        for(int k = 0; k < 3; ++k) {
+            if(!(p->range_max[k] > p->range_min[k])) return why = "rangeMax must exceed rangeMin", -1;
+        }
+    }
+    if(p->use_time_dependent_av && p->alpha_max < p->alpha_min) return why = "alphaMax < alphaMin", -1;
+    if(p->precision != SPHGPU_FP64 && p->precision != SPHGPU_MIXED) return why = "precision must be fp64 or mixed", -1;
+    return 0;
+}
+
+}  // namespace
+}  // namespace sphgpu
+
+using namespace sphgpu;
+
+extern "C" {
+
+void sphgpu_default_params(sphgpu_params* p)
+{
+    std::memset(p, 0, sizeof(*p));
+    p->sph_type = SPHGPU_SSPH;
+    p->kernel = SPHGPU_CUBIC_SPLINE;
+    p->neighbor_number = 50;
+    p->iterative_sml = 1;
+    p->gamma = 1.6666666666666667;
+    p->cfl_sound = 0.3;
+    p->cfl_force = 0.125;
+    p->av_alpha = 1.0;
+    p->use_balsara_switch = 1;
+    p->use_time_dependent_av = 0;
+    p->alpha_max = 2.0;
+    p->alpha_min = 0.1;
+    p->epsilon_av = 0.2;
+    p->use_ac = 0;
+    p->alpha_ac = 1.0;
+    p->max_tree_level = 20;
+    p->leaf_particle_num = 1;
+    p->periodic = 0;
+    p->use_gravity = 0;
+    p->g_constant = 1.0;
+    p->theta = 0.5;
+    p->gsph_2nd_order = 1;
+    p->riemann_solver = SPHGPU_RIEMANN_HLL;
+    p->precision = SPHGPU_FP64;
+    p->riemann_guess = SPHGPU_GUESS_NONE;
+    p->mlp_max_newton = 4;
+}
+
+int sphgpu_device_ok(void)
+{
+    int count = 0;
+    if(cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) return 0;
+    int dev = 0, major = 0;
+    if(cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess) return 0;
+    return major == 10 ? 1 : 0;
+}
+
+int sphgpu_create(const sphgpu_params* p, sphgpu_ctx** out)
+{
+    if(!p || !out) return SPHGPU_ERR_ARG;
+    *out = nullptr;
+    auto* c = new sphgpu_ctx;
+    c->prm = *p;
+    std::string why;
+    if(check_params(p, why)) {
+        c->err = why;
+        *out = c;
+        return SPHGPU_ERR_ARG;
+    }
+    set_dev_params(c);
+    *out = c;
+    if(!sphgpu_device_ok()) return fail(c, SPHGPU_ERR_CUDA, "no usable sm_100 CUDA device");
+    SPHGPU_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    for(int k = 0; k < 2; ++k) SPHGPU_CUDA(c, cudaEventCreate(&c->user_ev[k]));
+    return SPHGPU_OK;
+}
+
+int sphgpu_destroy(sphgpu_ctx* c)
+{
+    if(!c) return SPHGPU_OK;
+    if(c->stream) cudaStreamSynchronize(c->stream);
+    free_all(c);
+    if(c->d_mlp) cudaFree(c->d_mlp);
+    stage_flush(c);
+    for(cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+    for(cudaEvent_t e : c->user_ev) {
+        if(e) cudaEventDestroy(e);
+    }
+    if(c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return SPHGPU_OK;
+}
+
+const char* sphgpu_last_error(const sphgpu_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int sphgpu_upload(sphgpu_ctx* c, int64_t n, const double* const* fields)
+{
+    if(!c || n <= 0 || n > (1LL << 30)) return fail(c, SPHGPU_ERR_ARG, "particle count out of range");
+    if(!c->stream) return fail(c, SPHGPU_ERR_CUDA, "context has no device");
+    if((int)n != c->n || !c->s.pos) {
+        int rc = alloc_all(c, (int)n);
+        if(rc) return rc;
+    }
+    double* stage = nullptr;
+    SPHGPU_CUDA(c, cudaMallocAsync(&stage, sizeof(double) * (size_t)n, c->stream));
+    const unsigned g = grid_for(n, 256);
+    for(int f = 0; f < SPHGPU_NFIELDS; ++f) {
+        const double* src = fields ? fields[f] : nullptr;
+        if(src) SPHGPU_CUDA(c, cudaMemcpyAsync(stage, src, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+        const FieldRef r = field_ref(c->s, f);
+        if(r.comp == 4) k_put_nbr<<<g, 256, 0, c->stream>>>(c->s.nbr, src ? stage : nullptr, (int)n);
+        else k_put<<<g, 256, 0, c->stream>>>(r.arr, r.comp, src ? stage : nullptr, (int)n);
+    }
+    k_iota<<<g, 256, 0, c->stream>>>(c->s.id, (int)n);
+    SPHGPU_CUDA(c, cudaFreeAsync(stage, c->stream));
+    SPHGPU_LAUNCH_CHECK(c, "upload");
+    SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->have_tree = false;
+    c->first_pre = true;
+    c->time = 0.0;
+    return SPHGPU_OK;
+}
+
+int sphgpu_download(sphgpu_ctx* c, double* const* fields)
+{
+    if(!c || !fields) return SPHGPU_ERR_ARG;
+    if(c->n <= 0) return fail(c, SPHGPU_ERR_STATE, "no particles uploaded");
+    const int n = c->n;
+    double* stage = nullptr;
+    SPHGPU_CUDA(c, cudaMallocAsync(&stage, sizeof(double) * (size_t)n, c->stream));
+    const unsigned g = grid_for(n, 256);
+    for(int f = 0; f < SPHGPU_NFIELDS; ++f) {
+        if(!fields[f]) continue;
+        const FieldRef r = field_ref(c->s, f);
+        if(r.comp == 4) k_get_nbr<<<g, 256, 0, c->stream>>>(c->s.nbr, c->s.id, stage, n);
+        else k_get<<<g, 256, 0, c->stream>>>(r.arr, r.comp, c->s.id, stage, n);
+        SPHGPU_CUDA(c, cudaMemcpyAsync(fields[f], stage, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    }
+    SPHGPU_CUDA(c, cudaFreeAsync(stage, c->stream));
+    SPHGPU_LAUNCH_CHECK(c, "download");
+    SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    return SPHGPU_OK;
+}
+
+int64_t sphgpu_particle_num(const sphgpu_ctx* c) { return c ? c->n : 0; }
+
+int sphgpu_get_time(const sphgpu_ctx* c, double* time, double* dt)
+{
+    if(!c) return SPHGPU_ERR_ARG;
+    if(time) *time = c->time;
+    if(dt) {
+        if(!c->d_dt) {
+            *dt = 0.0;
+        } else {
+            cudaStreamSynchronize(c->stream);
+            if(cudaMemcpy(dt, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return SPHGPU_ERR_CUDA;
+        }
+    }
+    return SPHGPU_OK;
+}
+
+int sphgpu_set_dt(sphgpu_ctx* c, double dt)
+{
+    if(!c || !c->d_dt) return SPHGPU_ERR_ARG;
+    SPHGPU_CUDA(c, cudaMemcpyAsync(c->d_dt, &dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    return SPHGPU_OK;
+}
+
+int sphgpu_get_h_per_v_sig(const sphgpu_ctx* c, double* v)
+{
+    if(!c || !v || !c->d_hvs) return SPHGPU_ERR_ARG;
+    cudaStreamSynchronize(c->stream);
+    if(cudaMemcpy(v, c->d_hvs, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return SPHGPU_ERR_CUDA;
+    return SPHGPU_OK;
+}
+
+#define SPHGPU_NEED_STATE(c)                                                              \
+    do {                                                                                  \
+        if(!(c)) return SPHGPU_ERR_ARG;                                                   \
+        if((c)->n <= 0) return sphgpu::fail((c), SPHGPU_ERR_STATE, "no particles uploaded"); \
+    } while(0)
+
+int sphgpu_tree_make(sphgpu_ctx* c)
+{
+    SPHGPU_NEED_STATE(c);
+    return tree_make(c);
+}
+
+int sphgpu_tree_set_kernel(sphgpu_ctx* c)
+{
+    SPHGPU_NEED_STATE(c);
+    return tree_set_kernel(c);
+}
+
+int sphgpu_neighbor_search(sphgpu_ctx* c, int is_ij, int64_t* offsets, int32_t* ids, int64_t cap)
+{
+    SPHGPU_NEED_STATE(c);
+    if(!offsets) return SPHGPU_ERR_ARG;
+    const int rc = is_ij ? pair_walk(c) : gather_walk(c, false, 1.0);
+    if(rc < 0) return rc;
+    return export_lists(c, is_ij ? 1 : 0, offsets, ids, cap);
+}
+
+int sphgpu_exhaustive_search(sphgpu_ctx* c, int is_ij, int64_t* offsets, int32_t* ids, int64_t cap)
+{
+    SPHGPU_NEED_STATE(c);
+    if(!offsets) return SPHGPU_ERR_ARG;
+    return exhaustive_lists(c, is_ij, offsets, ids, cap);
+}
+
+int sphgpu_pre_interaction(sphgpu_ctx* c)
+{
+    SPHGPU_NEED_STATE(c);
+    return pre_interaction(c);
+}
+
+int sphgpu_fluid_force(sphgpu_ctx* c)
+{
+    SPHGPU_NEED_STATE(c);
+    return fluid_force(c);
+}
+
+int sphgpu_gravity_force(sphgpu_ctx* c)
+{
+    SPHGPU_NEED_STATE(c);
+    return gravity(c, false);
+}
+
+int sphgpu_gravity_direct(sphgpu_ctx* c)
+{
+    SPHGPU_NEED_STATE(c);
+    return gravity(c, true);
+}
+
+int sphgpu_timestep(sphgpu_ctx* c, double* dt)
+{
+    SPHGPU_NEED_STATE(c);
+    int rc = timestep(c);
+    if(rc < 0) return rc;
+    if(dt) {
+        SPHGPU_CUDA(c, cudaMemcpyAsync(dt, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    return SPHGPU_OK;
+}
+
+int sphgpu_predict(sphgpu_ctx* c)
+{
+    SPHGPU_NEED_STATE(c);
+    return predict(c);
+}
+
+int sphgpu_correct(sphgpu_ctx* c)
+{
+    SPHGPU_NEED_STATE(c);
+    return correct(c);
+}
+
+int sphgpu_initialize(sphgpu_ctx* c)
+{
+    SPHGPU_NEED_STATE(c);
+    // alpha = avAlpha, balsara = 1, sound = sqrt(gamma (gamma - 1) u)
+    k_init_state<<<grid_for(c->n, 256), 256, 0, c->stream>>>(c->s, c->n, c->prm.av_alpha,
+                                                             c->prm.gamma * (c->prm.gamma - 1.0));
+    SPHGPU_LAUNCH_CHECK(c, "initialize");
+    int rc = tree_make(c);
+    if(rc < 0) return rc;
+    rc = pre_interaction(c);
+    if(rc < 0) return rc;
+    rc = fluid_force(c);
+    if(rc < 0) return rc;
+    rc = gravity(c, false);
+    if(rc < 0) return rc;
+    SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    return SPHGPU_OK;
+}
+
+int sphgpu_integrate(sphgpu_ctx* c)
+{
+    SPHGPU_NEED_STATE(c);
+    int rc;
+    if((rc = timestep(c)) < 0) return rc;
+    double dt_h = 0.0;
+    SPHGPU_CUDA(c, cudaMemcpyAsync(&dt_h, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if((rc = predict(c)) < 0) return rc;
+    if((rc = tree_make(c)) < 0) return rc;
+    if((rc = pre_interaction(c)) < 0) return rc;
+    if((rc = fluid_force(c)) < 0) return rc;
+    if((rc = gravity(c, false)) < 0) return rc;
+    if((rc = correct(c)) < 0) return rc;
+    SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    stage_flush(c);
+    c->time += dt_h;
+    return SPHGPU_OK;
+}
+
+int sphgpu_energies(sphgpu_ctx* c, double* K, double* U, double* W, double* mom)
+{
+    SPHGPU_NEED_STATE(c);
+    double out[6];
+    const int rc = energies(c, out);
+    if(rc < 0) return rc;
+    if(K) *K = out[0];
+    if(U) *U = out[1];
+    if(W) *W = out[2];
+    if(mom) {
+        mom[0] = out[3];
+        mom[1] = out[4];
+        mom[2] = out[5];
+    }
+    return SPHGPU_OK;
+}
+
+int sphgpu_set_initial_smoothing(sphgpu_ctx* c, int on)
+{
+    if(!c) return SPHGPU_ERR_ARG;
+    c->first_pre = on != 0;
+    return SPHGPU_OK;
+}
+
+int64_t sphgpu_tree_nodes(sphgpu_ctx* c, int32_t* ints, double* dbl, int64_t cap)
+{
+    if(!c) return SPHGPU_ERR_ARG;
+    if(!c->have_tree) return fail(c, SPHGPU_ERR_STATE, "no tree");
+    const int64_t nn = c->node_count;
+    if(!ints || !dbl) return nn;
+    if(cap < nn) return fail(c, SPHGPU_ERR_ARG, "node buffer too small");
+    std::vector<int4> link((size_t)nn);
+    std::vector<double4> geo((size_t)nn), mass((size_t)nn);
+    std::vector<double> ks((size_t)nn);
+    SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    SPHGPU_CUDA(c, cudaMemcpy(link.data(), c->t.link, sizeof(int4) * nn, cudaMemcpyDeviceToHost));
+    SPHGPU_CUDA(c, cudaMemcpy(geo.data(), c->t.geo, sizeof(double4) * nn, cudaMemcpyDeviceToHost));
+    SPHGPU_CUDA(c, cudaMemcpy(mass.data(), c->t.mass, sizeof(double4) * nn, cudaMemcpyDeviceToHost));
+    SPHGPU_CUDA(c, cudaMemcpy(ks.data(), c->t.ksize, sizeof(double) * nn, cudaMemcpyDeviceToHost));
+    for(int64_t k = 0; k < nn; ++k) {
+        ints[3 * k] = link[k].w & 0xff;
+        ints[3 * k + 1] = (link[k].w >> 8) & 1;
+        ints[3 * k + 2] = link[k].y - link[k].x;
+        double* d = dbl + 9 * k;
+        d[0] = geo[k].x;
+        d[1] = geo[k].y;
+        d[2] = geo[k].z;
+        d[3] = geo[k].w;
+        d[4] = mass[k].w;
+        d[5] = mass[k].x;
+        d[6] = mass[k].y;
+        d[7] = mass[k].z;
+        d[8] = ks[k];
+    }
+    return nn;
+}
+
+int sphgpu_get_counters(sphgpu_ctx* c, sphgpu_counters* o)
+{
+    if(!c || !o) return SPHGPU_ERR_ARG;
+    std::memset(o, 0, sizeof(*o));
+    if(c->d_status) {
+        SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+        SPHGPU_CUDA(c, cudaMemcpy(&c->h_status, c->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost));
+    }
+    o->newton_nonconverged = (int64_t)c->h_status.newton_nonconv;
+    o->riemann_solves = (int64_t)c->h_status.riemann_solves;
+    o->riemann_iterations = (int64_t)c->h_status.riemann_iters;
+    o->riemann_fallbacks = (int64_t)c->h_status.riemann_fallbacks;
+    o->gather_capacity = c->gcap;
+    o->max_gather = c->max_gather;
+    o->max_pair = c->max_pair;
+    o->node_count = c->node_count;
+    o->retries = c->retries;
+    return SPHGPU_OK;
+}
+
+int sphgpu_reset_counters(sphgpu_ctx* c)
+{
+    if(!c) return SPHGPU_ERR_ARG;
+    if(c->d_status) {
+        SPHGPU_CUDA(c, cudaMemsetAsync(c->d_status, 0, sizeof(DevStatus), c->stream));
+        SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    std::memset(&c->h_status, 0, sizeof(c->h_status));
+    c->retries = 0;
+    return SPHGPU_OK;
+}
+
+int sphgpu_enable_timing(sphgpu_ctx* c, int on)
+{
+    if(!c) return SPHGPU_ERR_ARG;
+    if(c->stream) SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    stage_flush(c);
+    c->timing = on != 0;
+    c->launches = 0;
+    for(int k = 0; k < SPHGPU_NSTAGES; ++k) {
+        c->stage_ms[k] = 0.0;
+        c->stage_launch[k] = 0;
+    }
+    return SPHGPU_OK;
+}
+
+int sphgpu_get_stage_times(sphgpu_ctx* c, double* ms, int64_t* launches)
+{
+    if(!c || !ms) return SPHGPU_ERR_ARG;
+    if(c->stream) SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    stage_flush(c);
+    for(int k = 0; k < SPHGPU_NSTAGES; ++k) {
+        ms[k] = c->stage_ms[k];
+        if(launches) launches[k] = c->stage_launch[k];
+    }
+    return SPHGPU_OK;
+}
+
+int sphgpu_timer_start(sphgpu_ctx* c)
+{
+    if(!c || !c->stream) return SPHGPU_ERR_ARG;
+    SPHGPU_CUDA(c, cudaEventRecord(c->user_ev[0], c->stream));
+    return SPHGPU_OK;
+}
+
+int sphgpu_timer_stop(sphgpu_ctx* c, double* ms)
+{
+    if(!c || !c->stream || !ms) return SPHGPU_ERR_ARG;
+    SPHGPU_CUDA(c, cudaEventRecord(c->user_ev[1], c->stream));
+    SPHGPU_CUDA(c, cudaEventSynchronize(c->user_ev[1]));
+    float f = 0.f;
+    SPHGPU_CUDA(c, cudaEventElapsedTime(&f, c->user_ev[0], c->user_ev[1]));
+    *ms = f;
+    return SPHGPU_OK;
+}
+
+int64_t sphgpu_launch_count(const sphgpu_ctx* c) { return c ? c->launches : 0; }
+
+int sphgpu_synchronize(sphgpu_ctx* c)
+{
+    if(!c || !c->stream) return SPHGPU_ERR_ARG;
+    SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    return SPHGPU_OK;
+}
+
+}  // extern "C"

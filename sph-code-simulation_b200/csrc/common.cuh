@@ -1,0 +1,240 @@
+// common.cuh — device-side building blocks shared by every kernel file.
+//
+// Data layout in HBM (all arrays in octree / Morton order, length n).
+// Fields are packed four to a double4 by the stage that reads them together,
+// so a neighbour's inputs to a pair loop arrive in 32-byte sectors:
+//   pos    {x, y, z, mass}
+//   vel    {vx, vy, vz, sml}
+//   acc    {ax, ay, az, dene}
+//   velp   {vpx, vpy, vpz, ene_p}        (predictor half step)
+//   thermo {dens, pres, ene, sound}
+//   visc   {alpha, balsara, gradh, phi}
+//   grad   4 x n double4: GSPH MUSCL gradients of rho (3), P (3), v_x (3),
+//          v_y (3), v_z (3) packed in that order (15 used slots)
+//   id     int32  caller index of the particle (the reference's vector index)
+//   nbr    int32  neighbour count of the last PreInteraction
+// Octree nodes are stored in depth-first preorder (children in index order
+// 0..7, the order of BHNode::childs, include/bhtree.hpp:19-31) so a walk is a
+// forward scan with `skip` pointers over whole subtrees.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sphgpu.h"
+
+namespace sphgpu {
+
+constexpr unsigned FULL_MASK = 0xffffffffu;
+
+// ------------------------------------------------------------ parameters
+struct DevParams {
+    int sph_type, kernel, nngb, iterative;
+    double gamma, cfl_sound, cfl_force, av_alpha;
+    int balsara, td_av;
+    double alpha_max, alpha_min, eps_av;
+    int use_ac;
+    double alpha_ac;
+    int max_level, leaf_num;
+    int periodic;
+    double lo[3], hi[3], range[3];
+    int gravity;
+    double G, theta, theta2;
+    int gsph2, riemann, precision, guess, mlp_max_newton;
+    double ratio;  // kernel ratio 1.2 (iterative sml) or 1.0 (src/pre_interaction.cpp:31-35)
+};
+
+struct DevState {
+    int n;
+    double4* pos;
+    double4* vel;
+    double4* acc;
+    double4* velp;
+    double4* thermo;
+    double4* visc;
+    double4* grad;  // 4 * n
+    int* id;
+    int* nbr;
+};
+
+struct DevTree {
+    double4* geo;    // center x, y, z, edge
+    double4* mass;   // centre of mass x, y, z, mass
+    double* ksize;   // kernel_size: max sml in the subtree
+    int4* link;      // start, end, skip, level | is_leaf << 8
+    int* parent;
+    int* nchild;
+    int* counter;
+    int* nnodes;     // device scalar: total node count (root included)
+};
+
+// Packed status words read back by the host after a module.
+struct DevStatus {
+    int overflow;          // a neighbour list exceeded the current capacity
+    int fatal;             // a list exceeded neighbor_number * 1000
+    int max_count;         // largest list seen
+    int node_pool;         // node pool exhausted
+    int guard;             // a bounded device loop hit its limit (corrupt tree)
+    unsigned long long newton_nonconv;
+    unsigned long long riemann_solves;
+    unsigned long long riemann_iters;
+    unsigned long long riemann_fallbacks;
+};
+
+// Read-only 32-byte load through the non-coherent path (two 16-byte halves).
+__device__ __forceinline__ double4 ldg4(const double4* p)
+{
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const double2 a = __ldg(q), b = __ldg(q + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// ------------------------------------------------------------ exact FP64
+// The reference is compiled for x86-64 without FMA contraction; expressions
+// that decide set membership or tree topology use explicitly rounded
+// operations so they evaluate exactly as there.
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+
+// Periodic::calc_r_ij (include/periodic.hpp:34-59), one axis: candidates
+// d, d + L, d - L with the first minimal |.| winning ties.
+__device__ __forceinline__ double min_image(double d, double L)
+{
+    const double b = xadd(d, L), c = xsub(d, L);
+    const double ad = fabs(d), ab = fabs(b), ac = fabs(c);
+    if(ad <= ab && ad <= ac) return d;
+    if(ab <= ac && ab <= ad) return b;
+    if(ac <= ad && ac <= ab) return c;
+    return d;
+}
+
+struct Vec3d {
+    double x, y, z;
+};
+
+__device__ __forceinline__ Vec3d rij(const DevParams& P, double xi, double yi, double zi,
+                                     double xj, double yj, double zj)
+{
+    Vec3d d{xsub(xi, xj), xsub(yi, yj), xsub(zi, zj)};
+    if(P.periodic) {
+        d.x = min_image(d.x, P.range[0]);
+        d.y = min_image(d.y, P.range[1]);
+        d.z = min_image(d.z, P.range[2]);
+    }
+    return d;
+}
+
+// abs2 (include/vector_type.hpp:227-230): ((x*x + y*y) + z*z), unfused.
+__device__ __forceinline__ double abs2x(Vec3d d)
+{
+    return xadd(xadd(xmul(d.x, d.x), xmul(d.y, d.y)), xmul(d.z, d.z));
+}
+
+// ------------------------------------------------------------ SPH kernels
+// W, grad W (as the scalar c with grad W = r_ij c) and dW/dh for the cubic
+// spline (include/kernel/cubic_spline.hpp:21-53) and Wendland C4
+// (include/kernel/wendland_kernel.hpp:23-49), DIM = 3, restated from the
+// formulas; T = double (plain form) or float (mixed form).
+template <typename T>
+struct Kern {
+    static constexpr double PI = 3.14159265358979323846;
+    __device__ static __forceinline__ T cube(T x) { return x * x * x; }
+    __device__ static __forceinline__ T pow5(T x) { return x * x * x * x * x; }
+    __device__ static __forceinline__ T pow6(T x) { return x * x * x * x * x * x; }
+
+    __device__ static __forceinline__ T w(int type, T r, T h)
+    {
+        if(type == SPHGPU_WENDLAND) {
+            const T sigma = T(495.0 / (32.0 * PI));
+            const T q = r / h;
+            const T a = T(0.5) * (T(1) - q + fabs(T(1) - q));
+            return sigma / cube(h) * pow6(a) * (T(1) + T(6) * q + T(35.0 / 3.0) * q * q);
+        }
+        const T sigma = T(1.0 / PI);
+        const T hh = h * T(0.5);
+        const T q = r / hh;
+        const T a = T(0.5) * (T(2) - q + fabs(T(2) - q));
+        const T b = T(0.5) * (T(1) - q + fabs(T(1) - q));
+        return sigma / cube(hh) * (T(0.25) * cube(a) - cube(b));
+    }
+
+    __device__ static __forceinline__ T dwc(int type, T r, T h)
+    {
+        if(type == SPHGPU_WENDLAND) {
+            const T sigma = T(495.0 / (32.0 * PI));
+            const T q = r / h;
+            const T a = T(0.5) * (T(1) - q + fabs(T(1) - q));
+            return T(-56.0 / 3.0) * sigma / (cube(h) * (h * h)) * pow5(a) * (T(1) + T(5) * q);
+        }
+        if(r == T(0)) return T(0);
+        const T sigma = T(1.0 / PI);
+        const T hh = h * T(0.5);
+        const T q = r / hh;
+        const T a = T(0.5) * (T(2) - q + fabs(T(2) - q));
+        const T b = T(0.5) * (T(1) - q + fabs(T(1) - q));
+        return -sigma / (cube(hh) * hh * r) * (T(0.75) * (a * a) - T(3) * (b * b));
+    }
+
+    __device__ static __forceinline__ T dhw(int type, T r, T h)
+    {
+        if(type == SPHGPU_WENDLAND) {
+            const T sigma = T(495.0 / (32.0 * PI));
+            const T q = r / h;
+            const T a = T(0.5) * (T(1) - q + fabs(T(1) - q));
+            return -sigma / (cube(h) * h * T(3)) * pow5(a)
+                * (T(9) + T(45) * q + T(-5) * q * q - T(385) * cube(q));
+        }
+        const T sigma = T(1.0 / PI);
+        const T hh = h * T(0.5);
+        const T q = r / hh;
+        const T a = T(0.5) * (fabs(T(2) - q) + T(2) - q);
+        const T b = T(0.5) * (fabs(T(1) - q) + T(1) - q);
+        return T(0.5) * sigma / (cube(hh) * hh) * (a * a * (T(1.5) * q - T(1.5)) + b * b * (T(-6) * q + T(3)));
+    }
+};
+
+// ------------------------------------------------------------ reductions
+// Butterfly reductions over aligned groups of G lanes; every lane of the
+// warp must take part.  All lanes of a group end with the same bits.
+template <int G, typename T>
+__device__ __forceinline__ T group_sum(T v)
+{
+#pragma unroll
+    for(int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(FULL_MASK, v, o, G);
+    return v;
+}
+template <int G, typename T>
+__device__ __forceinline__ T group_max(T v)
+{
+#pragma unroll
+    for(int o = G / 2; o > 0; o >>= 1) {
+        const T u = __shfl_xor_sync(FULL_MASK, v, o, G);
+        v = u > v ? u : v;
+    }
+    return v;
+}
+template <typename T>
+__device__ __forceinline__ T warp_min(T v)
+{
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1) {
+        const T u = __shfl_xor_sync(FULL_MASK, v, o);
+        v = u < v ? u : v;
+    }
+    return v;
+}
+
+// Positive doubles order like their bit patterns.
+__device__ __forceinline__ void atomic_min_pos(double* addr, double v)
+{
+    atomicMin(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
+}
+__device__ __forceinline__ void atomic_max_pos(double* addr, double v)
+{
+    atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+inline unsigned grid_for(long long n, int block) { return (unsigned)((n + block - 1) / block); }
+
+}  // namespace sphgpu

@@ -1,0 +1,124 @@
+// context.cuh — the state behind one sphgpu_ctx: parameters, device arrays,
+// octree, neighbour lists, counters and stage timers.  One CUDA stream per
+// context; every module enqueues on it.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "scan_sort.cuh"
+
+struct sphgpu_ctx {
+    sphgpu_params prm{};
+    sphgpu::DevParams dp{};
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int n = 0;
+    bool have_tree = false;     // octree valid for the current positions
+    bool first_pre = true;      // PreInteraction::m_first (src/pre_interaction.cpp:41-44)
+    double time = 0.0;
+
+    // particle state (octree order) and its ping-pong copy for permutation
+    sphgpu::DevState s{}, alt{};
+    std::vector<void*> state_allocs;
+
+    // octree
+    sphgpu::DevTree t{};
+    int node_cap = 0;
+    double4* d_root = nullptr;       // root center x, y, z, edge
+    double* d_bbox_part = nullptr;   // per-block bbox partials
+    uint64_t *d_keys = nullptr, *d_keys_alt = nullptr;
+    uint32_t *d_vals = nullptr, *d_vals_alt = nullptr;
+    int* d_nstart = nullptr;         // nodes starting at particle p
+    int* d_base = nullptr;           // exclusive scan of d_nstart
+    int* d_lvl = nullptr;            // lfirst | leaf_level << 8
+    int* d_leaf_of_start = nullptr;  // leaf node index for node-starting particles, else -1
+    int* d_inv = nullptr;            // particle id -> octree position
+    void* d_radix_scratch = nullptr;
+    void* d_scan_scratch = nullptr;
+    sphgpu::ScanScratch scan{};
+
+    // neighbour lists (ELL: capacity slots per particle, row-major)
+    int* d_glist = nullptr;          // gather list (PreInteraction)
+    int* d_gcount = nullptr;
+    int64_t gcap = 0;
+    int* d_plist = nullptr;          // symmetric list (FluidForce)
+    int* d_pcount = nullptr;
+    int64_t pcap = 0;
+
+    // scalars
+    double* d_dt = nullptr;          // Simulation::dt
+    double* d_hvs = nullptr;         // Simulation::h_per_v_sig
+    double* d_red = nullptr;         // reduction scratch
+    sphgpu::DevStatus* d_status = nullptr;
+    sphgpu::DevStatus h_status{};
+
+    // learned Riemann guess (BF16 weights + FP32 biases on device)
+    void* d_mlp = nullptr;
+    bool have_mlp = false;
+    std::vector<float> mlp_master;
+
+    // counters kept on the host
+    int64_t retries = 0;
+    int64_t max_gather = 0, max_pair = 0, node_count = 0;
+
+    // timing: event pairs recorded around each stage and read back at the
+    // next point where the host waits on the stream anyway
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    struct Pending {
+        int stage;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    cudaEvent_t open_ev[SPHGPU_NSTAGES] = {};
+    double stage_ms[SPHGPU_NSTAGES] = {};
+    int64_t stage_launch[SPHGPU_NSTAGES] = {};
+    int64_t launches = 0;          // kernels launched by this context
+    cudaEvent_t user_ev[2] = {};   // sphgpu_timer_start / stop
+};
+
+namespace sphgpu {
+
+// errors
+int fail(sphgpu_ctx* c, int code, const std::string& msg);
+int cuda_fail(sphgpu_ctx* c, cudaError_t e, const char* where);
+
+#define SPHGPU_CUDA(c, call)                                   \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if(e_ != cudaSuccess) return cuda_fail((c), e_, #call); \
+    } while(0)
+
+#define SPHGPU_LAUNCH_CHECK(c, where)                             \
+    do {                                                          \
+        cudaError_t e_ = cudaGetLastError();                      \
+        if(e_ != cudaSuccess) return cuda_fail((c), e_, (where)); \
+    } while(0)
+
+// stage timers
+void stage_begin(sphgpu_ctx* c, int stage);
+void stage_end(sphgpu_ctx* c, int stage, int launches);
+void stage_flush(sphgpu_ctx* c);   // call only after the stream is idle
+
+// module implementations (each returns an sphgpu_status)
+int tree_make(sphgpu_ctx* c);
+int tree_set_kernel(sphgpu_ctx* c);
+int gather_walk(sphgpu_ctx* c, bool compute_guess, double ratio);
+int pair_walk(sphgpu_ctx* c);
+int export_lists(sphgpu_ctx* c, int which, int64_t* offsets, int32_t* ids, int64_t cap);
+int exhaustive_lists(sphgpu_ctx* c, int is_ij, int64_t* offsets, int32_t* ids, int64_t cap);
+int pre_interaction(sphgpu_ctx* c);
+int fluid_force(sphgpu_ctx* c);
+int gravity(sphgpu_ctx* c, bool direct);
+int timestep(sphgpu_ctx* c);
+int predict(sphgpu_ctx* c);
+int correct(sphgpu_ctx* c);
+int energies(sphgpu_ctx* c, double* out5 /* K, U, W, px.. */);
+int read_status(sphgpu_ctx* c);
+int ensure_list_capacity(sphgpu_ctx* c, int which, int64_t cap);
+
+}  // namespace sphgpu

@@ -1,0 +1,206 @@
+// gravity.cu — GravityForce::calculation (Barnes–Hut tree walk and the
+// exhaustive direct sum).
+//
+// Reference: src/gravity_force.cpp:52-89, BHNode::calc_force
+// (src/bhtree.cpp:347-393) and the Hernquist & Katz softening kernels f, g
+// (src/bhtree.cpp:318-345).
+//
+// Warp-cooperative walk over the preorder node array: a warp owns 32
+// consecutive particles (octree order); each lane keeps a bit per tree level
+// saying "I opened my level-L ancestor".  At a node that is live for a lane
+// the lane either accepts it as an (unsoftened) monopole, or opens it — a leaf
+// is then summed pairwise with spline-softened f and g, an internal node is
+// descended into (the warp descends when any lane opened).  Each lane meets
+// its nodes in exactly the order of the reference's recursion and adds into
+// acc (starting from the fluid acceleration) in that order, so in the plain
+// form with unfused FP64 (-fmad=false for this file) the result is
+// bit-identical to the reference's on the same tree.
+// T = float (mixed form): distances, opening test and kernels in FP32, the
+// per-particle acc / phi accumulators in FP64.
+#include <cuda_runtime.h>
+
+#include "context.cuh"
+
+namespace sphgpu {
+
+namespace {
+
+constexpr int GBLK = 128;
+
+// Hernquist & Katz (1989) potential / force kernels (src/bhtree.cpp:318-345)
+template <typename T>
+__device__ __forceinline__ T hk_f(T r, T h)
+{
+    const T e = h * T(0.5);
+    const T u = r / e;
+    if(u < T(1.0)) return (T(-0.5) * u * u * (T(1.0 / 3.0) - T(3.0 / 20) * u * u + u * u * u / T(20)) + T(1.4)) / e;
+    if(u < T(2.0))
+        return T(-1.0) / (T(15) * r) + (-u * u * (T(4.0 / 3.0) - u + T(0.3) * u * u - u * u * u / T(30)) + T(1.6)) / e;
+    return T(1) / r;
+}
+
+template <typename T>
+__device__ __forceinline__ T hk_g(T r, T h)
+{
+    const T e = h * T(0.5);
+    const T u = r / e;
+    if(u < T(1.0)) return (T(4.0 / 3.0) - T(1.2) * u * u + T(0.5) * u * u * u) / (e * e * e);
+    if(u < T(2.0))
+        return (T(-1.0 / 15) + T(8.0 / 3) * u * u * u - T(3) * u * u * u * u + T(1.2) * u * u * u * u * u
+                - u * u * u * u * u * u / T(6.0))
+            / (r * r * r);
+    return T(1) / (r * r * r);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(GBLK) k_gravity(DevParams P, DevState S, DevTree Tr, int n,
+                                                  DevStatus* __restrict__ st)
+{
+    const int i = blockIdx.x * GBLK + threadIdx.x;
+    const bool valid = i < n;
+    double xi = 0, yi = 0, zi = 0, hi = 1;
+    double4 acc = make_double4(0, 0, 0, 0);
+    if(valid) {
+        const double4 p = S.pos[i];
+        xi = p.x;
+        yi = p.y;
+        zi = p.z;
+        hi = S.vel[i].w;
+        acc = S.acc[i];
+    }
+    double ax = acc.x, ay = acc.y, az = acc.z, phi = 0.0;
+    const double G = P.G;
+    const T theta2 = (T)P.theta2;
+    const int nnodes = *Tr.nnodes;
+    unsigned bits = 0;
+    int nd = 0, steps = 0;
+    while(nd < nnodes) {
+        if(++steps > nnodes) {  // corrupt node table: report, never loop
+            st->guard = 1;
+            break;
+        }
+        const int4 lk = __ldg(&Tr.link[nd]);
+        const int L = lk.w & 0xff;
+        const bool leaf = (lk.w >> 8) != 0;
+        const unsigned need = (1u << L) - 2u;
+        bool open = false;
+        if(valid && (bits & need) == need) {
+            const double edge = ldg4(&Tr.geo[nd]).w;
+            const double4 mc = ldg4(&Tr.mass[nd]);
+            const Vec3d d = rij(P, xi, yi, zi, mc.x, mc.y, mc.z);
+            if(sizeof(T) == sizeof(double)) {
+                const double l2 = edge * edge;
+                const double d2 = d.x * d.x + d.y * d.y + d.z * d.z;
+                open = (l2 > P.theta2 * d2) || (d2 < l2);
+                if(!open) {
+                    const double rinv = 1.0 / sqrt(d2);
+                    phi -= G * mc.w * rinv;
+                    const double s = G * mc.w * (rinv * rinv * rinv);
+                    ax -= d.x * s;
+                    ay -= d.y * s;
+                    az -= d.z * s;
+                }
+            } else {
+                const float dx = (float)d.x, dy = (float)d.y, dz = (float)d.z;
+                const float l2 = (float)edge * (float)edge;
+                const float d2 = dx * dx + dy * dy + dz * dz;
+                open = (l2 > (float)theta2 * d2) || (d2 < l2);
+                if(!open) {
+                    const float rinv = rsqrtf(d2);
+                    const float gm = (float)(G * mc.w);
+                    phi -= (double)(gm * rinv);
+                    const float s = gm * (rinv * rinv * rinv);
+                    ax -= (double)(dx * s);
+                    ay -= (double)(dy * s);
+                    az -= (double)(dz * s);
+                }
+            }
+            if(open && leaf) {
+                for(int q = lk.x; q < lk.y; ++q) {
+                    if(q == i) continue;
+                    const double4 pq = ldg4(&S.pos[q]);
+                    const double hq = ldg4(&S.vel[q]).w;
+                    const Vec3d r = rij(P, xi, yi, zi, pq.x, pq.y, pq.z);
+                    if(sizeof(T) == sizeof(double)) {
+                        const double rr = sqrt(r.x * r.x + r.y * r.y + r.z * r.z);
+                        phi -= G * pq.w * (hk_f<double>(rr, hi) + hk_f<double>(rr, hq)) * 0.5;
+                        const double c = G * pq.w * (hk_g<double>(rr, hi) + hk_g<double>(rr, hq)) * 0.5;
+                        ax -= r.x * c;
+                        ay -= r.y * c;
+                        az -= r.z * c;
+                    } else {
+                        const float rx = (float)r.x, ry = (float)r.y, rz = (float)r.z;
+                        const float rr = sqrtf(rx * rx + ry * ry + rz * rz);
+                        const float gm = (float)(G * pq.w);
+                        phi -= (double)(gm * (hk_f<float>(rr, (float)hi) + hk_f<float>(rr, (float)hq)) * 0.5f);
+                        const float c = gm * (hk_g<float>(rr, (float)hi) + hk_g<float>(rr, (float)hq)) * 0.5f;
+                        ax -= (double)(rx * c);
+                        ay -= (double)(ry * c);
+                        az -= (double)(rz * c);
+                    }
+                }
+            }
+        }
+        if(leaf) {
+            nd = lk.z;
+        } else {
+            bits = open ? (bits | (1u << L)) : (bits & ~(1u << L));
+            nd = __any_sync(FULL_MASK, open) ? nd + 1 : lk.z;
+        }
+    }
+    if(valid) {
+        S.acc[i] = make_double4(ax, ay, az, acc.w);
+        S.visc[i].w = phi;
+    }
+}
+
+// -DEXHAUSTIVE_SEARCH direct summation (src/gravity_force.cpp:70-84): every j
+// in caller-index order, self included.
+__global__ void k_gravity_direct(DevParams P, DevState S, int n, const int* __restrict__ inv)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const double4 p = S.pos[i];
+    const double hi = S.vel[i].w;
+    const double G = P.G;
+    double phi = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
+    for(int jid = 0; jid < n; ++jid) {
+        const int j = inv[jid];
+        const double4 pj = S.pos[j];
+        const double hj = S.vel[j].w;
+        const Vec3d r = rij(P, p.x, p.y, p.z, pj.x, pj.y, pj.z);
+        const double rr = sqrt(r.x * r.x + r.y * r.y + r.z * r.z);
+        phi -= G * pj.w * (hk_f<double>(rr, hi) + hk_f<double>(rr, hj)) * 0.5;
+        const double c = G * pj.w * (hk_g<double>(rr, hi) + hk_g<double>(rr, hj)) * 0.5;
+        fx -= r.x * c;
+        fy -= r.y * c;
+        fz -= r.z * c;
+    }
+    double4 a = S.acc[i];
+    a.x += fx;
+    a.y += fy;
+    a.z += fz;
+    S.acc[i] = a;
+    S.visc[i].w = phi;
+}
+
+}  // namespace
+
+int gravity(sphgpu_ctx* c, bool direct)
+{
+    if(!c->prm.use_gravity) return SPHGPU_OK;
+    if(!direct && !c->have_tree) return fail(c, SPHGPU_ERR_STATE, "GravityForce before tree make");
+    stage_begin(c, SPHGPU_T_GRAVITY);
+    if(direct) {
+        k_gravity_direct<<<grid_for(c->n, 128), 128, 0, c->stream>>>(c->dp, c->s, c->n, c->d_inv);
+    } else if(c->prm.precision == SPHGPU_MIXED) {
+        k_gravity<float><<<grid_for(c->n, GBLK), GBLK, 0, c->stream>>>(c->dp, c->s, c->t, c->n, c->d_status);
+    } else {
+        k_gravity<double><<<grid_for(c->n, GBLK), GBLK, 0, c->stream>>>(c->dp, c->s, c->t, c->n, c->d_status);
+    }
+    SPHGPU_LAUNCH_CHECK(c, "GravityForce");
+    stage_end(c, SPHGPU_T_GRAVITY, 1);
+    return SPHGPU_OK;
+}
+
+}  // namespace sphgpu

@@ -1,0 +1,278 @@
+// walk.cu — batched BHTree::neighbor_search and exhaustive_search.
+//
+// Reference: BHNode::neighbor_search (src/bhtree.cpp:277-316) — per node, the
+// L-infinity box test |d_k| <= edge/2 + h against the node centre, then at a
+// leaf the radius test r^2 < h^2 on every particle of the leaf list, with
+// h = sml (gather) or max(sml, node.kernel_size) (is_ij).
+//
+// Warp-cooperative walk: a warp owns 32 consecutive particles in octree order
+// (spatially coherent) and scans the preorder node array once.  Each lane
+// keeps one bit per tree level: bit L says "my box test passed at the current
+// level-L ancestor".  A node at level L is live for a lane iff bits 1..L-1 are
+// all set — exactly the set of nodes the reference's recursion would visit
+// for that particle.  The warp descends into a node (index + 1) when any live
+// lane passes, else jumps over the subtree (skip pointer).  Every test is
+// evaluated in unfused FP64 (this file builds with -fmad=false) so each
+// lane's list equals the reference's list as a set, and even in order before
+// the reference's distance sort.
+//
+// Lists go to an ELL buffer (capacity slots per particle, row-major).  A list
+// longer than the capacity is counted but not stored; the host grows the
+// buffer and re-runs (status.overflow).  More than neighbor_number * 1000
+// entries is the reference's fatal overflow (src/bhtree.cpp:129-135).
+#include <cuda_runtime.h>
+
+#include "context.cuh"
+
+namespace sphgpu {
+
+namespace {
+
+constexpr int WBLK = 128;
+
+template <bool IJ>
+__global__ void __launch_bounds__(WBLK) k_walk(DevParams P, DevState S, DevTree T, int n, int cap,
+                                               int* __restrict__ list, int* __restrict__ count,
+                                               DevStatus* __restrict__ st, int guess, double ratio)
+{
+    const int i = blockIdx.x * WBLK + threadIdx.x;
+    const bool valid = i < n;
+    double xi = 0, yi = 0, zi = 0, hi = 0;
+    if(valid) {
+        const double4 p = S.pos[i];
+        xi = p.x;
+        yi = p.y;
+        zi = p.z;
+        if(guess) {
+            // h guess from the previous density (src/pre_interaction.cpp:61-64)
+            constexpr double A = 4.0 * 3.14159265358979323846 / 3.0;
+            const double dens = S.thermo[i].x;
+            hi = pow(P.nngb * p.w / (dens * A), 1.0 / 3) * ratio;
+            S.vel[i].w = hi;
+        } else {
+            hi = S.vel[i].w;
+        }
+    }
+    const int nnodes = *T.nnodes;
+    const size_t row = (size_t)i * (size_t)cap;
+    int cnt = 0;
+    unsigned bits = 0;
+    int nd = 0, steps = 0;
+    while(nd < nnodes) {
+        // a preorder scan visits each node at most once; more means a corrupt
+        // node table: stop and report instead of looping
+        if(++steps > nnodes) {
+            st->guard = 1;
+            break;
+        }
+        const int4 lk = __ldg(&T.link[nd]);
+        const double4 g = ldg4(&T.geo[nd]);
+        const int L = lk.w & 0xff;
+        const bool leaf = (lk.w >> 8) != 0;
+        const unsigned need = (1u << L) - 2u;
+        bool pass = false;
+        double h2 = 0.0;
+        if(valid && (bits & need) == need) {
+            double h = hi;
+            if(IJ) {
+                const double ks = __ldg(&T.ksize[nd]);
+                h = hi < ks ? ks : hi;
+            }
+            h2 = h * h;
+            const double l2 = (g.w * 0.5 + h) * (g.w * 0.5 + h);
+            const Vec3d d = rij(P, xi, yi, zi, g.x, g.y, g.z);
+            double m = d.x * d.x;
+            const double m1 = d.y * d.y, m2 = d.z * d.z;
+            if(m1 > m) m = m1;
+            if(m2 > m) m = m2;
+            pass = m <= l2;
+        }
+        if(leaf) {
+            if(pass) {
+                for(int q = lk.x; q < lk.y; ++q) {
+                    const double4 pq = ldg4(&S.pos[q]);
+                    const Vec3d r = rij(P, xi, yi, zi, pq.x, pq.y, pq.z);
+                    if(abs2x(r) < h2) {
+                        if(cnt < cap) list[row + cnt] = q;
+                        ++cnt;
+                    }
+                }
+            }
+            nd = lk.z;
+        } else {
+            bits = pass ? (bits | (1u << L)) : (bits & ~(1u << L));
+            nd = __any_sync(FULL_MASK, pass) ? nd + 1 : lk.z;
+        }
+    }
+    if(valid) {
+        count[i] = cnt;
+        if(cnt > cap) st->overflow = 1;
+        if(cnt > P.nngb * 1000) st->fatal = 1;
+        atomicMax(&st->max_count, cnt);
+    }
+}
+
+// exhaustive_search (src/exhaustive_search.cpp:11-42): all j with
+// r^2 < h_i^2 (gather) or r^2 < max(h_i^2, h_j^2) (is_ij).
+__global__ void k_exhaustive(DevParams P, DevState S, int n, int is_ij, int cap, int* __restrict__ list,
+                             int* __restrict__ count, DevStatus* __restrict__ st)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const double4 p = S.pos[i];
+    const double hi = S.vel[i].w;
+    const double ki2 = hi * hi;
+    int cnt = 0;
+    for(int j = 0; j < n; ++j) {
+        const double4 pj = S.pos[j];
+        const Vec3d r = rij(P, p.x, p.y, p.z, pj.x, pj.y, pj.z);
+        const double r2 = abs2x(r);
+        double lim = ki2;
+        if(is_ij) {
+            const double hj = S.vel[j].w;
+            const double kj2 = hj * hj;
+            lim = ki2 < kj2 ? kj2 : ki2;
+        }
+        if(r2 < lim) {
+            if(cnt < cap) list[(size_t)i * cap + cnt] = j;
+            ++cnt;
+        }
+    }
+    count[i] = cnt;
+    if(cnt > cap) st->overflow = 1;
+    if(cnt > P.nngb * 1000) st->fatal = 1;
+    atomicMax(&st->max_count, cnt);
+}
+
+__global__ void k_counts_by_id(int n, const int* __restrict__ id, const int* __restrict__ count,
+                               unsigned long long* __restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < n) out[id[i]] = (unsigned long long)count[i];
+}
+
+__global__ void k_fill_by_id(int n, int cap, const int* __restrict__ id, const int* __restrict__ count,
+                             const int* __restrict__ list, const unsigned long long* __restrict__ off,
+                             int* __restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const unsigned long long b = off[id[i]];
+    const int c = count[i];
+    for(int k = 0; k < c; ++k) out[b + k] = id[list[(size_t)i * cap + k]];
+}
+
+int run_walk(sphgpu_ctx* c, int which, bool guess, double ratio, bool exhaustive, int is_ij, int* launches)
+{
+    cudaStream_t st = c->stream;
+    const int n = c->n;
+    for(int attempt = 0; attempt < 4; ++attempt) {
+        ++*launches;
+        const int64_t cap = which == 0 ? c->gcap : c->pcap;
+        int* list = which == 0 ? c->d_glist : c->d_plist;
+        int* count = which == 0 ? c->d_gcount : c->d_pcount;
+        SPHGPU_CUDA(c, cudaMemsetAsync(c->d_status, 0, 3 * sizeof(int), st));
+        SPHGPU_CUDA(c, cudaMemsetAsync(&c->d_status->guard, 0, sizeof(int), st));
+        if(exhaustive) {
+            k_exhaustive<<<grid_for(n, 128), 128, 0, st>>>(c->dp, c->s, n, is_ij, (int)cap, list, count, c->d_status);
+        } else if(which == 0) {
+            k_walk<false><<<grid_for(n, WBLK), WBLK, 0, st>>>(c->dp, c->s, c->t, n, (int)cap, list, count,
+                                                            c->d_status, guess ? 1 : 0, ratio);
+        } else {
+            k_walk<true><<<grid_for(n, WBLK), WBLK, 0, st>>>(c->dp, c->s, c->t, n, (int)cap, list, count,
+                                                           c->d_status, 0, 1.0);
+        }
+        SPHGPU_LAUNCH_CHECK(c, "neighbour walk");
+        SPHGPU_CUDA(c, cudaMemcpyAsync(&c->h_status, c->d_status, 5 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        SPHGPU_CUDA(c, cudaStreamSynchronize(st));
+        if(c->h_status.fatal) {
+            return fail(c, SPHGPU_ERR_NEIGHBOR_OVERFLOW,
+                        "Neighbor list overflow: more than neighborNumber * 1000 neighbours");
+        }
+        if(c->h_status.guard) return fail(c, SPHGPU_ERR_STATE, "tree walk exceeded the node count (corrupt tree)");
+        if(which == 0) c->max_gather = c->h_status.max_count;
+        else c->max_pair = c->h_status.max_count;
+        if(!c->h_status.overflow) return attempt == 0 ? SPHGPU_OK : SPHGPU_RETRIED;
+        // grow to the largest list seen (+12.5%, rounded to 32) and re-run;
+        // a guessed h is recomputed identically on the re-run
+        int64_t want = c->h_status.max_count + c->h_status.max_count / 8;
+        want = (want + 31) / 32 * 32;
+        const int rc = ensure_list_capacity(c, which, want);
+        if(rc < 0) return rc;
+        ++c->retries;
+    }
+    return fail(c, SPHGPU_ERR_NEIGHBOR_OVERFLOW, "neighbour list capacity did not converge");
+}
+
+}  // namespace
+
+int gather_walk(sphgpu_ctx* c, bool compute_guess, double ratio)
+{
+    if(!c->have_tree) return fail(c, SPHGPU_ERR_STATE, "neighbour search before tree make");
+    stage_begin(c, SPHGPU_T_GATHER_WALK);
+    int launches = 0;
+    const int rc = run_walk(c, 0, compute_guess, ratio, false, 0, &launches);
+    stage_end(c, SPHGPU_T_GATHER_WALK, launches);
+    return rc;
+}
+
+int pair_walk(sphgpu_ctx* c)
+{
+    if(!c->have_tree) return fail(c, SPHGPU_ERR_STATE, "neighbour search before tree make");
+    stage_begin(c, SPHGPU_T_PAIR_WALK);
+    int launches = 0;
+    const int rc = run_walk(c, 1, false, 1.0, false, 1, &launches);
+    stage_end(c, SPHGPU_T_PAIR_WALK, launches);
+    return rc;
+}
+
+// Copy list `which` (0 gather, 1 pair) to a host CSR in caller order with
+// caller ids.
+int export_lists(sphgpu_ctx* c, int which, int64_t* offsets, int32_t* ids, int64_t cap)
+{
+    cudaStream_t st = c->stream;
+    const int n = c->n;
+    const int64_t lcap = which == 0 ? c->gcap : c->pcap;
+    const int* list = which == 0 ? c->d_glist : c->d_plist;
+    const int* count = which == 0 ? c->d_gcount : c->d_pcount;
+    unsigned long long *d_cnt = nullptr, *d_off = nullptr, *d_tot = nullptr;
+    SPHGPU_CUDA(c, cudaMallocAsync(&d_cnt, sizeof(unsigned long long) * (size_t)(2 * n + 2), st));
+    d_off = d_cnt + n;
+    d_tot = d_off + n;
+    k_counts_by_id<<<grid_for(n, 256), 256, 0, st>>>(n, c->s.id, count, d_cnt);
+    exclusive_scan(d_cnt, d_off, n, d_tot, c->scan, st);
+    unsigned long long total = 0;
+    SPHGPU_CUDA(c, cudaMemcpyAsync(&total, d_tot, sizeof(total), cudaMemcpyDeviceToHost, st));
+    std::vector<unsigned long long> off(n);
+    SPHGPU_CUDA(c, cudaMemcpyAsync(off.data(), d_off, sizeof(unsigned long long) * (size_t)n,
+                                   cudaMemcpyDeviceToHost, st));
+    SPHGPU_CUDA(c, cudaStreamSynchronize(st));
+    for(int i = 0; i < n; ++i) offsets[i] = (int64_t)off[i];
+    offsets[n] = (int64_t)total;
+    int rc = SPHGPU_OK;
+    if(ids) {
+        if((int64_t)total > cap) {
+            rc = fail(c, SPHGPU_ERR_ARG, "neighbour id buffer too small");
+        } else {
+            int* d_ids = nullptr;
+            SPHGPU_CUDA(c, cudaMallocAsync(&d_ids, sizeof(int) * (size_t)(total + 1), st));
+            k_fill_by_id<<<grid_for(n, 256), 256, 0, st>>>(n, (int)lcap, c->s.id, count, list, d_off, d_ids);
+            SPHGPU_CUDA(c, cudaMemcpyAsync(ids, d_ids, sizeof(int) * (size_t)total, cudaMemcpyDeviceToHost, st));
+            SPHGPU_CUDA(c, cudaFreeAsync(d_ids, st));
+        }
+    }
+    SPHGPU_CUDA(c, cudaFreeAsync(d_cnt, st));
+    SPHGPU_CUDA(c, cudaStreamSynchronize(st));
+    return rc;
+}
+
+int exhaustive_lists(sphgpu_ctx* c, int is_ij, int64_t* offsets, int32_t* ids, int64_t cap)
+{
+    int launches = 0;
+    const int rc = run_walk(c, 1, false, 1.0, true, is_ij, &launches);
+    c->launches += launches;
+    if(rc < 0) return rc;
+    return export_lists(c, 1, offsets, ids, cap);
+}
+
+}  // namespace sphgpu

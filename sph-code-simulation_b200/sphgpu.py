@@ -1,0 +1,398 @@
+"""Python binding of the C ABI in include/sphgpu.h (ctypes).
+
+Mirrors the reference's module surface over a GPU context:
+
+    sim = Simulation(params)            # Simulation(param) + BHTree::initialize
+    sim.upload(fields)                  # particle arrays, caller order
+    sim.initialize()                    # tail of Solver::initialize
+    sim.integrate()                     # Solver::integrate + update_time
+    sim.tree_make(); sim.pre_interaction(); sim.fluid_force(); ...
+
+Errors from the library raise :class:`SPHException` (the reference's
+THROW_ERROR -> sph::SPHException convention, include/exception.hpp:9-14).
+There is no CPU fallback: loading fails loudly when libsphgpu.so is absent,
+and compute calls fail when no sm_100 device is present.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict, Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsphgpu.so")
+
+# enums (include/sphgpu.h)
+SSPH, DISPH, GSPH = 0, 1, 2
+CUBIC_SPLINE, WENDLAND = 0, 1
+RIEMANN_HLL, RIEMANN_ITERATIVE = 0, 1
+FP64, MIXED = 0, 1
+GUESS_NONE, GUESS_MLP = 0, 1
+
+FIELDS = [
+    "pos_x", "pos_y", "pos_z", "vel_x", "vel_y", "vel_z", "velp_x", "velp_y", "velp_z",
+    "acc_x", "acc_y", "acc_z", "mass", "dens", "pres", "ene", "ene_p", "dene", "sml", "sound",
+    "balsara", "alpha", "gradh", "phi", "neighbor",
+    "grad_d_x", "grad_d_y", "grad_d_z", "grad_p_x", "grad_p_y", "grad_p_z",
+    "grad_v0_x", "grad_v0_y", "grad_v0_z", "grad_v1_x", "grad_v1_y", "grad_v1_z",
+    "grad_v2_x", "grad_v2_y", "grad_v2_z",
+]
+NFIELDS = len(FIELDS)
+FIELD_INDEX = {f: k for k, f in enumerate(FIELDS)}
+STAGES = ["timestep", "predict", "tree", "gather_walk", "pre", "set_kernel", "pair_walk",
+          "force", "gravity", "correct"]
+
+
+class SPHException(RuntimeError):
+    """Raised for fatal (<0) status codes of the C ABI."""
+
+
+class Params(C.Structure):
+    """sphgpu_params (include/sphgpu.h); field names follow the JSON keys."""
+
+    _fields_ = [
+        ("sph_type", C.c_int32), ("kernel", C.c_int32), ("neighbor_number", C.c_int32),
+        ("iterative_sml", C.c_int32), ("gamma", C.c_double), ("cfl_sound", C.c_double),
+        ("cfl_force", C.c_double), ("av_alpha", C.c_double), ("use_balsara_switch", C.c_int32),
+        ("use_time_dependent_av", C.c_int32), ("alpha_max", C.c_double), ("alpha_min", C.c_double),
+        ("epsilon_av", C.c_double), ("use_ac", C.c_int32), ("max_tree_level", C.c_int32),
+        ("alpha_ac", C.c_double), ("leaf_particle_num", C.c_int32), ("periodic", C.c_int32),
+        ("range_min", C.c_double * 3), ("range_max", C.c_double * 3), ("use_gravity", C.c_int32),
+        ("gsph_2nd_order", C.c_int32), ("g_constant", C.c_double), ("theta", C.c_double),
+        ("riemann_solver", C.c_int32), ("precision", C.c_int32), ("riemann_guess", C.c_int32),
+        ("mlp_max_newton", C.c_int32),
+    ]
+
+    def copy(self) -> "Params":
+        p = Params()
+        C.memmove(C.byref(p), C.byref(self), C.sizeof(Params))
+        return p
+
+    def as_dict(self) -> Dict:
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if name.startswith("range_") else v
+        return out
+
+
+class Counters(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in (
+        "newton_nonconverged", "riemann_solves", "riemann_iterations", "riemann_fallbacks",
+        "gather_capacity", "max_gather", "max_pair", "node_count", "retries")]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libsphgpu.so (built in-tree by build.py); raise if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run __graft_entry__.build() first")
+    L = C.CDLL(LIB_PATH)
+    vp, i64, i32p, i64p, dp = C.c_void_p, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_double)
+    dpp = C.POINTER(C.POINTER(C.c_double))
+    sig = {
+        "sphgpu_default_params": (None, [C.POINTER(Params)]),
+        "sphgpu_create": (C.c_int, [C.POINTER(Params), C.POINTER(vp)]),
+        "sphgpu_destroy": (C.c_int, [vp]),
+        "sphgpu_last_error": (C.c_char_p, [vp]),
+        "sphgpu_device_ok": (C.c_int, []),
+        "sphgpu_upload": (C.c_int, [vp, i64, dpp]),
+        "sphgpu_download": (C.c_int, [vp, dpp]),
+        "sphgpu_particle_num": (i64, [vp]),
+        "sphgpu_get_time": (C.c_int, [vp, dp, dp]),
+        "sphgpu_set_dt": (C.c_int, [vp, C.c_double]),
+        "sphgpu_get_h_per_v_sig": (C.c_int, [vp, dp]),
+        "sphgpu_tree_make": (C.c_int, [vp]),
+        "sphgpu_tree_set_kernel": (C.c_int, [vp]),
+        "sphgpu_neighbor_search": (C.c_int, [vp, C.c_int, i64p, i32p, i64]),
+        "sphgpu_exhaustive_search": (C.c_int, [vp, C.c_int, i64p, i32p, i64]),
+        "sphgpu_pre_interaction": (C.c_int, [vp]),
+        "sphgpu_fluid_force": (C.c_int, [vp]),
+        "sphgpu_gravity_force": (C.c_int, [vp]),
+        "sphgpu_gravity_direct": (C.c_int, [vp]),
+        "sphgpu_timestep": (C.c_int, [vp, dp]),
+        "sphgpu_predict": (C.c_int, [vp]),
+        "sphgpu_correct": (C.c_int, [vp]),
+        "sphgpu_initialize": (C.c_int, [vp]),
+        "sphgpu_integrate": (C.c_int, [vp]),
+        "sphgpu_energies": (C.c_int, [vp, dp, dp, dp, dp]),
+        "sphgpu_get_counters": (C.c_int, [vp, C.POINTER(Counters)]),
+        "sphgpu_reset_counters": (C.c_int, [vp]),
+        "sphgpu_enable_timing": (C.c_int, [vp, C.c_int]),
+        "sphgpu_get_stage_times": (C.c_int, [vp, dp, i64p]),
+        "sphgpu_synchronize": (C.c_int, [vp]),
+        "sphgpu_set_initial_smoothing": (C.c_int, [vp, C.c_int]),
+        "sphgpu_tree_nodes": (i64, [vp, i32p, dp, i64]),
+        "sphgpu_mlp_param_count": (i64, []),
+        "sphgpu_mlp_set_params": (C.c_int, [vp, C.POINTER(C.c_float)]),
+        "sphgpu_mlp_get_params": (C.c_int, [vp, C.POINTER(C.c_float)]),
+        "sphgpu_sample_evrard": (i64, [C.c_int, C.c_double, C.c_double, dpp]),
+        "sphgpu_sample_shear_layer": (i64, [C.c_double, C.c_double, C.c_double, dpp]),
+        "sphgpu_sample_shock_tube": (i64, [C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, dpp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def default_params(**kw) -> Params:
+    p = Params()
+    lib().sphgpu_default_params(C.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        if k.startswith("range_"):
+            setattr(p, k, (C.c_double * 3)(*v))
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def device_ok() -> bool:
+    return bool(lib().sphgpu_device_ok())
+
+
+def _field_ptrs(arrays: Dict[str, np.ndarray], n: int, writable: bool):
+    ptrs = (C.POINTER(C.c_double) * NFIELDS)()
+    keep = []
+    for name, arr in arrays.items():
+        k = FIELD_INDEX[name]
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.shape != (n,):
+            raise ValueError(f"field {name}: shape {a.shape} != ({n},)")
+        if writable and a is not arr:
+            raise ValueError(f"field {name} must be a contiguous float64 array")
+        keep.append(a)
+        ptrs[k] = a.ctypes.data_as(C.POINTER(C.c_double))
+    return ptrs, keep
+
+
+def _sample(fn, *args) -> Dict[str, np.ndarray]:
+    n = fn(*args, None)
+    out = {f: np.zeros(n) for f in FIELDS}
+    ptrs, _ = _field_ptrs(out, n, True)
+    fn(*args, ptrs)
+    return out
+
+
+def sample_evrard(N: int, G: float = 1.0, gamma: float = 5.0 / 3.0) -> Dict[str, np.ndarray]:
+    """Evrard sphere on an N^3 lattice (Solver::make_evrard, src/sample/evrard.cpp:13-87)."""
+    return _sample(lib().sphgpu_sample_evrard, C.c_int(N), C.c_double(G), C.c_double(gamma))
+
+
+def sample_shear_layer(dx: float, lz: float = 0.125, gamma: float = 5.0 / 3.0) -> Dict[str, np.ndarray]:
+    """3-D periodic shear layer (Kelvin-Helmholtz set-up of src/sample/khi.cpp:12-73, extruded)."""
+    return _sample(lib().sphgpu_sample_shear_layer, C.c_double(dx), C.c_double(lz), C.c_double(gamma))
+
+
+def sample_shock_tube(dx: float, ly: float = 0.05, p_left: float = 1000.0, p_right: float = 0.01,
+                      gamma: float = 1.4) -> Dict[str, np.ndarray]:
+    """3-D shock tube along x in [-0.5, 0.5] x [0, ly]^2."""
+    return _sample(lib().sphgpu_sample_shock_tube, C.c_double(dx), C.c_double(ly), C.c_double(p_left),
+                   C.c_double(p_right), C.c_double(gamma))
+
+
+class Simulation:
+    """A GPU context: Simulation + BHTree + the per-step modules."""
+
+    def __init__(self, params: Params):
+        self.params = params.copy()
+        self._h = C.c_void_p()
+        rc = lib().sphgpu_create(C.byref(self.params), C.byref(self._h))
+        if rc < 0:
+            msg = self._err()
+            lib().sphgpu_destroy(self._h)
+            self._h = C.c_void_p()
+            raise SPHException(f"sphgpu_create failed ({rc}): {msg}")
+        self.n = 0
+
+    # ---- lifetime
+    def close(self):
+        if self._h:
+            lib().sphgpu_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _err(self) -> str:
+        e = lib().sphgpu_last_error(self._h)
+        return e.decode() if e else ""
+
+    def _check(self, rc: int, what: str) -> int:
+        if rc < 0:
+            raise SPHException(f"{what} failed ({rc}): {self._err()}")
+        return rc
+
+    # ---- state
+    def upload(self, fields: Dict[str, np.ndarray]):
+        n = len(next(iter(fields.values())))
+        ptrs, keep = _field_ptrs({k: v for k, v in fields.items() if k in FIELD_INDEX}, n, False)
+        self._check(lib().sphgpu_upload(self._h, n, ptrs), "upload")
+        self.n = n
+        del keep
+
+    def download(self, names=None) -> Dict[str, np.ndarray]:
+        names = list(FIELDS) if names is None else list(names)
+        out = {f: np.zeros(self.n) for f in names}
+        ptrs, _ = _field_ptrs(out, self.n, True)
+        self._check(lib().sphgpu_download(self._h, ptrs), "download")
+        return out
+
+    def time_dt(self):
+        t, dt = C.c_double(), C.c_double()
+        self._check(lib().sphgpu_get_time(self._h, C.byref(t), C.byref(dt)), "get_time")
+        return t.value, dt.value
+
+    def set_dt(self, dt: float):
+        self._check(lib().sphgpu_set_dt(self._h, dt), "set_dt")
+
+    def h_per_v_sig(self) -> float:
+        v = C.c_double()
+        self._check(lib().sphgpu_get_h_per_v_sig(self._h, C.byref(v)), "h_per_v_sig")
+        return v.value
+
+    # ---- modules
+    def tree_make(self):
+        return self._check(lib().sphgpu_tree_make(self._h), "BHTree::make")
+
+    def set_kernel(self):
+        return self._check(lib().sphgpu_tree_set_kernel(self._h), "BHTree::set_kernel")
+
+    def neighbor_search(self, is_ij: bool = False, exhaustive: bool = False):
+        """All particles' lists (radius sml) as a CSR (offsets[n+1], ids) in caller order."""
+        off = np.zeros(self.n + 1, dtype=np.int64)
+        fn = lib().sphgpu_exhaustive_search if exhaustive else lib().sphgpu_neighbor_search
+        i64p, i32p = C.POINTER(C.c_int64), C.POINTER(C.c_int32)
+        self._check(fn(self._h, int(is_ij), off.ctypes.data_as(i64p), None, 0), "neighbor_search")
+        ids = np.zeros(max(int(off[-1]), 1), dtype=np.int32)
+        self._check(fn(self._h, int(is_ij), off.ctypes.data_as(i64p), ids.ctypes.data_as(i32p), ids.size),
+                    "neighbor_search")
+        return off, ids[: int(off[-1])]
+
+    def pre_interaction(self):
+        return self._check(lib().sphgpu_pre_interaction(self._h), "PreInteraction::calculation")
+
+    def fluid_force(self):
+        return self._check(lib().sphgpu_fluid_force(self._h), "FluidForce::calculation")
+
+    def gravity_force(self, direct: bool = False):
+        fn = lib().sphgpu_gravity_direct if direct else lib().sphgpu_gravity_force
+        return self._check(fn(self._h), "GravityForce::calculation")
+
+    def timestep(self) -> float:
+        dt = C.c_double()
+        self._check(lib().sphgpu_timestep(self._h, C.byref(dt)), "TimeStep::calculation")
+        return dt.value
+
+    def predict(self):
+        return self._check(lib().sphgpu_predict(self._h), "predict")
+
+    def correct(self):
+        return self._check(lib().sphgpu_correct(self._h), "correct")
+
+    def initialize(self):
+        return self._check(lib().sphgpu_initialize(self._h), "initialize")
+
+    def integrate(self):
+        return self._check(lib().sphgpu_integrate(self._h), "integrate")
+
+    def energies(self):
+        k, u, w = C.c_double(), C.c_double(), C.c_double()
+        mom = (C.c_double * 3)()
+        self._check(lib().sphgpu_energies(self._h, C.byref(k), C.byref(u), C.byref(w),
+                                          C.cast(mom, C.POINTER(C.c_double))), "energies")
+        return k.value, u.value, w.value, np.array(mom[:])
+
+    def set_initial_smoothing(self, on: bool):
+        self._check(lib().sphgpu_set_initial_smoothing(self._h, int(on)), "set_initial_smoothing")
+
+    def tree_nodes(self):
+        """Preorder node table: ints (level, is_leaf, num), dbl (center3, edge, mass, mcenter3, ksize)."""
+        k = self._check(lib().sphgpu_tree_nodes(self._h, None, None, 0), "tree_nodes")
+        ints = np.zeros((k, 3), dtype=np.int32)
+        dbl = np.zeros((k, 9), dtype=np.float64)
+        self._check(lib().sphgpu_tree_nodes(self._h, ints.ctypes.data_as(C.POINTER(C.c_int32)),
+                                            dbl.ctypes.data_as(C.POINTER(C.c_double)), k), "tree_nodes")
+        return ints, dbl
+
+    # ---- diagnostics
+    def counters(self) -> Dict[str, int]:
+        c = Counters()
+        self._check(lib().sphgpu_get_counters(self._h, C.byref(c)), "counters")
+        return {n: getattr(c, n) for n, _ in Counters._fields_}
+
+    def reset_counters(self):
+        self._check(lib().sphgpu_reset_counters(self._h), "reset_counters")
+
+    def enable_timing(self, on: bool = True):
+        self._check(lib().sphgpu_enable_timing(self._h, int(on)), "enable_timing")
+
+    def stage_times(self):
+        ms = (C.c_double * len(STAGES))()
+        la = (C.c_int64 * len(STAGES))()
+        self._check(lib().sphgpu_get_stage_times(self._h, C.cast(ms, C.POINTER(C.c_double)),
+                                                 C.cast(la, C.POINTER(C.c_int64))), "stage_times")
+        return {s: (ms[k], la[k]) for k, s in enumerate(STAGES)}
+
+    def synchronize(self):
+        self._check(lib().sphgpu_synchronize(self._h), "synchronize")
+
+    # ---- learned Riemann guess
+    def mlp_set_params(self, params: np.ndarray):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        if p.size != lib().sphgpu_mlp_param_count():
+            raise ValueError("wrong MLP parameter count")
+        self._check(lib().sphgpu_mlp_set_params(self._h, p.ctypes.data_as(C.POINTER(C.c_float))), "mlp_set_params")
+
+    def mlp_get_params(self) -> np.ndarray:
+        p = np.zeros(lib().sphgpu_mlp_param_count(), dtype=np.float32)
+        self._check(lib().sphgpu_mlp_get_params(self._h, p.ctypes.data_as(C.POINTER(C.c_float))), "mlp_get_params")
+        return p
+
+
+def config_params(name: str, **overrides) -> Params:
+    """Parameters of the benchmark workloads (names describe the workload)."""
+    if name == "evrard_ssph":          # ssph Evrard sphere, cubic spline, K=50, leaf=1
+        p = default_params(sph_type=SSPH, kernel=CUBIC_SPLINE, neighbor_number=50, use_balsara_switch=1,
+                           av_alpha=1.0, use_gravity=1, g_constant=1.0, theta=0.5, leaf_particle_num=1,
+                           gamma=5.0 / 3.0, cfl_sound=0.3)
+    elif name == "shear_disph":        # disph periodic shear layer, Wendland, K=128, AC
+        p = default_params(sph_type=DISPH, kernel=WENDLAND, neighbor_number=128, use_ac=1, alpha_ac=1.0,
+                           periodic=1, range_min=(0.0, 0.0, 0.0), range_max=(1.0, 1.0, 0.125),
+                           gamma=5.0 / 3.0)
+    elif name == "tube_gsph":          # gsph shock tube, MUSCL, iterative Riemann, cubic, K=50
+        p = default_params(sph_type=GSPH, kernel=CUBIC_SPLINE, neighbor_number=50, gsph_2nd_order=1,
+                           riemann_solver=RIEMANN_ITERATIVE, gamma=1.4, periodic=1,
+                           range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.05, 0.05))
+    elif name == "evrard_disph":       # disph + gravity sphere, Wendland, K=128, TD-AV, AC
+        p = default_params(sph_type=DISPH, kernel=WENDLAND, neighbor_number=128, use_time_dependent_av=1,
+                           alpha_min=0.1, alpha_max=2.0, epsilon_av=0.2, use_balsara_switch=1, use_ac=1,
+                           alpha_ac=1.0, use_gravity=1, g_constant=1.0, theta=0.5, gamma=5.0 / 3.0)
+    else:
+        raise KeyError(name)
+    for k, v in overrides.items():
+        if k.startswith("range_"):
+            setattr(p, k, (C.c_double * 3)(*v))
+        else:
+            setattr(p, k, v)
+    return p

@@ -1,0 +1,169 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+Run in a container where the reference sources are mounted (default
+/root/reference, override with REFDIR) after `make -C oracle`:
+
+    python tests/golden/make_golden.py
+
+What it writes (all produced by the reference's own compiled modules,
+oracle/_ref/libsphref*.so, driven by oracle/ref_harness.cpp):
+
+  evrard_t0.npz      The reference's shipped Evrard t=0 snapshot
+                     (sample/evrard/results_new/00000.dat, energy.dat row t=0;
+                     configuration sample/evrard/evrard.json: N=30 lattice,
+                     ssph, Wendland, neighborNumber=32, leafParticleNumber=32,
+                     Balsara + time-dependent AV, G=1).  The script recomputes
+                     it with the compiled reference and asserts agreement to the
+                     printed 6 digits, then stores every 16th particle's printed
+                     row, the recomputed full-precision values for the same
+                     particles, and W0.
+  steps_<cfg>.npz    Small instances of the four benchmark workloads: the
+                     full particle state after Solver::initialize and after
+                     each of two Solver::integrate steps, plus dt.
+  lists_<cfg>.npz    Distance-sorted neighbour lists (CSR) from
+                     BHTree::neighbor_search and from exhaustive_search
+                     (gather and is_ij) at the state after initialize.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, "sph-code-simulation_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import oracle as O  # noqa: E402
+import sphgpu as G  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+REFDIR = os.environ.get("REFDIR", "/root/reference")
+
+STATE_FIELDS = ["pos_x", "pos_y", "pos_z", "vel_x", "vel_y", "vel_z", "acc_x", "acc_y", "acc_z", "mass",
+                "dens", "pres", "ene", "dene", "sml", "sound", "balsara", "alpha", "gradh", "phi", "neighbor",
+                "velp_x", "velp_y", "velp_z", "ene_p",
+                "grad_d_x", "grad_d_y", "grad_d_z", "grad_p_x", "grad_p_y", "grad_p_z",
+                "grad_v0_x", "grad_v0_y", "grad_v0_z", "grad_v1_x", "grad_v1_y", "grad_v1_z",
+                "grad_v2_x", "grad_v2_y", "grad_v2_z"]
+
+# small instances of the benchmark workloads (name, params, sample)
+SMALL = {
+    "evrard_ssph": (lambda: G.config_params("evrard_ssph"), lambda: G.sample_evrard(12)),
+    "evrard_disph": (lambda: G.config_params("evrard_disph", neighbor_number=64),
+                     lambda: G.sample_evrard(12)),
+    "tube_gsph": (lambda: G.config_params("tube_gsph", range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.1, 0.1)),
+                  lambda: G.sample_shock_tube(0.025, ly=0.1)),
+    "tube_gsph_hll": (lambda: G.config_params("tube_gsph", riemann_solver=G.RIEMANN_HLL,
+                                              range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.1, 0.1)),
+                      lambda: G.sample_shock_tube(0.025, ly=0.1)),
+    "shear_disph": (lambda: G.config_params("shear_disph", neighbor_number=64),
+                    lambda: G.sample_shear_layer(0.05, lz=0.125)),
+}
+
+
+def evrard_golden():
+    p = G.default_params(sph_type=G.SSPH, kernel=G.WENDLAND, neighbor_number=32, leaf_particle_num=32,
+                         use_balsara_switch=1, use_time_dependent_av=1, av_alpha=1.0, use_ac=0,
+                         use_gravity=1, g_constant=1.0, gamma=1.66666666666666666667, cfl_sound=0.2,
+                         cfl_force=0.1)
+    fields = G.sample_evrard(30)
+    ref = O.Reference(p, fields)
+    ref.initialize()
+    st = ref.download()
+    k, u, w, _ = ref.energies()
+    shipped = np.loadtxt(os.path.join(REFDIR, "sample/evrard/results_new/00000.dat"), comments="#")
+    ids = shipped[:, 14].astype(int)
+    order = np.argsort(ids)
+    shipped = shipped[order]
+    assert len(shipped) == len(fields["pos_x"]) == 14328
+    cols = {"pos_x": 0, "pos_y": 1, "pos_z": 2, "acc_x": 6, "acc_y": 7, "acc_z": 8, "mass": 9, "dens": 10,
+            "pres": 11, "ene": 12, "sml": 13, "neighbor": 15, "alpha": 16, "gradh": 17}
+    worst = 0.0
+    for f, c in cols.items():
+        ref_v = st[f]
+        printed = shipped[:, c]
+        rel = np.abs(ref_v - printed) / np.maximum(np.abs(printed), 1e-300)
+        # 6 significant digits printed; tiny components compared absolutely
+        tol = 6e-6 * np.maximum(np.abs(printed), 1e-6 * np.max(np.abs(printed)))
+        bad = np.abs(ref_v - printed) > tol
+        assert not bad.any(), (f, np.flatnonzero(bad)[:5])
+        worst = max(worst, float(np.max(rel[np.abs(printed) > 1e-3 * np.max(np.abs(printed))])))
+    energy = np.loadtxt(os.path.join(REFDIR, "sample/evrard/results_new/energy.dat"), comments="#")
+    w0_printed = energy[0, 3]
+    assert abs(w - w0_printed) < 1e-6, (w, w0_printed)
+    sel = np.arange(0, len(shipped), 16)
+    np.savez_compressed(
+        os.path.join(OUT, "evrard_t0.npz"),
+        ids=sel,
+        printed=shipped[sel],
+        printed_columns=np.array(list(cols.keys())),
+        printed_index=np.array(list(cols.values())),
+        **{"ref_" + f: st[f][sel] for f in cols},
+        ref_phi=st["phi"][sel],
+        w0_printed=w0_printed,
+        w0_ref=w,
+        k0_ref=k,
+        u0_ref=u,
+    )
+    print(f"evrard_t0: 14328 particles match 00000.dat to 6 digits (worst rel {worst:.2e}); W0 {w:.9f}")
+
+
+def small_steps(name, steps=2):
+    mkp, mks = SMALL[name]
+    p = mkp()
+    fields = mks()
+    ref = O.Reference(p, fields)
+    ref.initialize()
+    states = [ref.download(STATE_FIELDS)]
+    dts = [0.0]
+    for _ in range(steps):
+        ref.integrate()
+        states.append(ref.download(STATE_FIELDS))
+        dts.append(ref.dt)
+    out = {"n": len(fields["pos_x"]), "dt": np.array(dts), "params": np.frombuffer(bytes(p), dtype=np.uint8)}
+    for k in ("pos_x", "pos_y", "pos_z", "vel_x", "vel_y", "vel_z", "mass", "dens", "pres", "ene"):
+        out["ic_" + k] = fields[k]
+    for s, st in enumerate(states):
+        for f, v in st.items():
+            out[f"s{s}_{f}"] = v
+    np.savez_compressed(os.path.join(OUT, f"steps_{name}.npz"), **out)
+    print(f"steps_{name}: n={out['n']} dt={dts}")
+    return p, fields
+
+
+def lists(name):
+    mkp, mks = SMALL[name]
+    p = mkp()
+    fields = mks()
+    out = {}
+    for exh in (False, True):
+        ref = O.Reference(p, fields, exhaustive=exh)
+        ref.initialize()
+        st = ref.download(STATE_FIELDS)
+        tag = "exh" if exh else "tree"
+        for is_ij in (0, 1):
+            off, ids = ref.neighbor_lists(bool(is_ij))
+            out[f"{tag}_ij{is_ij}_off"] = off
+            out[f"{tag}_ij{is_ij}_ids"] = ids
+        if not exh:
+            for f, v in st.items():
+                out["state_" + f] = v
+    np.savez_compressed(os.path.join(OUT, f"lists_{name}.npz"), **out)
+    print(f"lists_{name}: {len(out['tree_ij0_ids'])} gather / {len(out['tree_ij1_ids'])} pair entries")
+
+
+def main():
+    O.build(reference=True)
+    if not O.have_reference():
+        raise SystemExit("reference libraries not built; is REFDIR mounted?")
+    evrard_golden()
+    for name in SMALL:
+        small_steps(name)
+    for name in ("evrard_ssph", "tube_gsph", "shear_disph"):
+        lists(name)
+
+
+if __name__ == "__main__":
+    main()

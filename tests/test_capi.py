@@ -1,0 +1,66 @@
+"""The C-ABI library: loads without a GPU, exports every declared symbol,
+mirrors the reference's parameter defaults, fails loudly without a device."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "sphgpu.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = set(re.findall(r"\b(sphgpu_\w+)\s*\(", src))
+    return sorted(names)
+
+
+def test_exports_every_declared_symbol(G):
+    lib = G.lib()
+    names = _declared()
+    assert len(names) >= 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_default_params_match_reference_defaults(G):
+    """Defaults of Solver::read_parameterfile (src/solver.cpp:311-438)."""
+    p = G.default_params()
+    assert p.neighbor_number == 50 and p.leaf_particle_num == 1 and p.max_tree_level == 20
+    assert p.cfl_sound == 0.3 and p.cfl_force == 0.125 and p.av_alpha == 1.0
+    assert p.use_balsara_switch == 1 and p.iterative_sml == 1 and p.theta == 0.5
+    assert p.gsph_2nd_order == 1 and p.riemann_solver == G.RIEMANN_HLL
+    assert p.alpha_max == 2.0 and p.alpha_min == 0.1 and p.epsilon_av == 0.2
+    assert p.gamma == pytest.approx(5.0 / 3.0, rel=1e-15)
+
+
+def test_params_struct_layout(G):
+    import ctypes
+    # offsets of the C struct (natural alignment), checked against ctypes
+    assert ctypes.sizeof(G.Params) == 192
+
+
+def test_samples(G):
+    ev = G.sample_evrard(32)
+    assert len(ev["pos_x"]) == 17256
+    r = np.sqrt(ev["pos_x"] ** 2 + ev["pos_y"] ** 2 + ev["pos_z"] ** 2)
+    assert r.max() <= 1.0 and np.allclose(ev["mass"].sum(), 1.0)
+    sh = G.sample_shear_layer(0.05)
+    assert np.all((sh["pos_y"] > 0.25) & (sh["pos_y"] < 0.75) == (sh["dens"] == 2.0))
+    tu = G.sample_shock_tube(0.025, ly=0.1)
+    assert np.all((tu["pos_x"] < 0) == (tu["pres"] == 1000.0))
+
+
+def test_create_without_device_fails_loudly(G):
+    if G.device_ok():
+        pytest.skip("a device is present")
+    with pytest.raises(G.SPHException):
+        G.Simulation(G.default_params())
+
+
+def test_bad_params_rejected(G):
+    with pytest.raises(G.SPHException, match="maxTreeLevel"):
+        G.Simulation(G.default_params(max_tree_level=30))
+    with pytest.raises(G.SPHException, match="kernel"):
+        G.Simulation(G.default_params(kernel=7))

@@ -1,0 +1,117 @@
+"""The CPU restatement (oracle/) against the reference's own outputs.
+
+Fixtures in tests/golden/ were produced by the reference's compiled modules
+(tests/golden/make_golden.py); evrard_t0 additionally carries rows of the
+reference's shipped snapshot sample/evrard/results_new/00000.dat.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden, params_from_bytes
+
+SMALL = ["evrard_ssph", "evrard_disph", "tube_gsph", "tube_gsph_hll", "shear_disph"]
+
+
+def _fields_from_ic(g):
+    n = int(g["n"])
+    f = {k[3:]: g[k] for k in g.files if k.startswith("ic_")}
+    assert len(f["pos_x"]) == n
+    return f
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_oracle_matches_reference_steps(G, O, name):
+    """Bit-identical particle state after initialize and two integrate steps."""
+    g = golden(f"steps_{name}.npz")
+    p = params_from_bytes(G, g["params"])
+    o = O.Oracle(p, _fields_from_ic(g))
+    o.initialize()
+    for s in range(3):
+        st = o.download()
+        for f in g.files:
+            if not f.startswith(f"s{s}_"):
+                continue
+            name_f = f[len(f"s{s}_"):]
+            np.testing.assert_array_equal(st[name_f], g[f], err_msg=f"step {s} field {name_f}")
+        if s > 0:
+            assert o.dt == g["dt"][s]
+        if s < 2:
+            o.integrate()
+
+
+def test_oracle_evrard_t0_golden(G, O):
+    """Shipped Evrard t=0 snapshot (N=30, Wendland, K=32, leaf=32, TD-AV)."""
+    g = golden("evrard_t0.npz")
+    p = G.default_params(sph_type=G.SSPH, kernel=G.WENDLAND, neighbor_number=32, leaf_particle_num=32,
+                         use_balsara_switch=1, use_time_dependent_av=1, av_alpha=1.0, use_gravity=1,
+                         g_constant=1.0, gamma=1.66666666666666666667, cfl_sound=0.2, cfl_force=0.1)
+    o = O.Oracle(p, G.sample_evrard(30))
+    o.initialize()
+    st = o.download()
+    ids = g["ids"]
+    for col, idx in zip(g["printed_columns"], g["printed_index"]):
+        np.testing.assert_array_equal(st[str(col)][ids], g["ref_" + str(col)], err_msg=str(col))
+        printed = g["printed"][:, idx]
+        tol = 6e-6 * np.maximum(np.abs(printed), 1e-6 * np.max(np.abs(printed)))
+        assert np.all(np.abs(st[str(col)][ids] - printed) <= tol), col
+    k, u, w, _ = o.energies()
+    assert w == pytest.approx(float(g["w0_ref"]), rel=1e-13)
+    assert abs(w - float(g["w0_printed"])) < 1e-6
+
+
+@pytest.mark.parametrize("name", ["evrard_ssph", "tube_gsph", "shear_disph"])
+def test_oracle_neighbor_lists(G, O, name):
+    """Distance-sorted lists equal the reference's tree and exhaustive lists."""
+    g = golden(f"lists_{name}.npz")
+    s = golden(f"steps_{name}.npz")
+    p = params_from_bytes(G, s["params"])
+    fields = {k[len("state_"):]: g[k] for k in g.files if k.startswith("state_")}
+    for exh in (False, True):
+        o = O.Oracle(p, fields, exhaustive=exh)
+        if not exh:
+            o.tree_make()
+            o.set_kernel()
+        tag = "exh" if exh else "tree"
+        for ij in (0, 1):
+            off, ids = o.neighbor_lists(bool(ij))
+            np.testing.assert_array_equal(off, g[f"{tag}_ij{ij}_off"])
+            np.testing.assert_array_equal(ids, g[f"{tag}_ij{ij}_ids"])
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_kernel_derivatives(O, kind):
+    """dW/dr and dW/dh against central differences (test/kernel_test/kernel_test.cpp:8-85)."""
+    prev = None
+    for n in (100, 200, 400, 800):
+        dx = 1.0 / n
+        xs = np.arange(dx * 0.5, 1.0, dx)
+        e_r = np.mean([abs(O.kernel_dwc(kind, x, 1.0) * x
+                           - (O.kernel_w(kind, x + dx / 2, 1.0) - O.kernel_w(kind, x - dx / 2, 1.0)) / dx)
+                       for x in xs])
+        e_h = np.mean([abs(O.kernel_dhw(kind, x, 1.0)
+                           - (O.kernel_w(kind, x, 1.0 + dx / 2) - O.kernel_w(kind, x, 1.0 - dx / 2)) / dx)
+                       for x in xs])
+        assert e_r < 5e-3 and e_h < 5e-3
+        if prev is not None:
+            assert e_r <= prev[0] * 0.6 + 1e-12 and e_h <= prev[1] * 0.6 + 1e-12
+        prev = (e_r, e_h)
+
+
+def test_kernel_normalisation(O):
+    """4 pi int_0^h W r^2 dr = 1 for both kernels."""
+    r = np.linspace(0, 1, 20001)
+    for kind in (0, 1):
+        w = np.array([O.kernel_w(kind, x, 1.0) for x in r])
+        assert np.trapezoid(4 * np.pi * r * r * w, r) == pytest.approx(1.0, rel=1e-6)
+
+
+def test_riemann_solvers(O):
+    """Identical states give p* = p, v* = u; a Sod-like state converges."""
+    for solver in (0, 1):
+        p, v, _ = O.riemann(solver, (0.3, 1.0, 2.0, 1.5), (0.3, 1.0, 2.0, 1.5), 1.4)
+        assert p == pytest.approx(2.0, rel=1e-6) and v == pytest.approx(0.3, rel=1e-6)
+    p, v, it = O.riemann(1, (0.0, 1.0, 1.0, np.sqrt(1.4)), (0.0, 0.125, 0.1, np.sqrt(1.4 * 0.8)), 1.4)
+    assert 1 <= it <= 20
+    assert 0.25 < p < 0.35 and 0.8 < v < 1.0  # exact Sod star state p*=0.3031, u*=0.9274
+    p, v, it = O.riemann(1, (0.0, -1.0, 1.0, 1.0), (0.0, 1.0, 1.0, 1.0), 1.4)
+    assert (p, v, it) == (0.0, 0.0, 0)
