@@ -195,21 +195,33 @@ struct Kern {
 };
 
 // ------------------------------------------------------------ reductions
-// Butterfly reductions over aligned groups of G lanes; every lane of the
-// warp must take part.  All lanes of a group end with the same bits.
+// Butterfly reductions over an aligned group of G lanes.  The shuffle mask
+// names only the group's own lanes: groups of one warp may leave a loop at
+// different iterations (per-particle Newton convergence), so a warp-wide
+// mask would wait for lanes that never arrive.  All lanes of a group take
+// identical control flow and end with the same bits.
+template <int G>
+__device__ __forceinline__ unsigned group_mask()
+{
+    if(G == 32) return FULL_MASK;
+    const unsigned lane = threadIdx.x & 31u;
+    return ((1u << G) - 1u) << (lane & ~(unsigned)(G - 1));
+}
 template <int G, typename T>
 __device__ __forceinline__ T group_sum(T v)
 {
+    const unsigned m = group_mask<G>();
 #pragma unroll
-    for(int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(FULL_MASK, v, o, G);
+    for(int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(m, v, o, G);
     return v;
 }
 template <int G, typename T>
 __device__ __forceinline__ T group_max(T v)
 {
+    const unsigned m = group_mask<G>();
 #pragma unroll
     for(int o = G / 2; o > 0; o >>= 1) {
-        const T u = __shfl_xor_sync(FULL_MASK, v, o, G);
+        const T u = __shfl_xor_sync(m, v, o, G);
         v = u > v ? u : v;
     }
     return v;
