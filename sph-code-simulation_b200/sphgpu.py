@@ -129,6 +129,9 @@ def lib() -> C.CDLL:
         "sphgpu_get_stage_times": (C.c_int, [vp, dp, i64p]),
         "sphgpu_synchronize": (C.c_int, [vp]),
         "sphgpu_set_initial_smoothing": (C.c_int, [vp, C.c_int]),
+        "sphgpu_timer_start": (C.c_int, [vp]),
+        "sphgpu_timer_stop": (C.c_int, [vp, dp]),
+        "sphgpu_launch_count": (i64, [vp]),
         "sphgpu_tree_nodes": (i64, [vp, i32p, dp, i64]),
         "sphgpu_mlp_param_count": (i64, []),
         "sphgpu_mlp_set_params": (C.c_int, [vp, C.POINTER(C.c_float)]),
