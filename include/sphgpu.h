@@ -244,6 +244,17 @@ int64_t sphgpu_mlp_param_count(void);
 int sphgpu_mlp_set_params(sphgpu_ctx* ctx, const float* params);
 int sphgpu_mlp_get_params(sphgpu_ctx* ctx, float* params);
 
+/* ---------------- workload generators (inputs, not the hot path) ------- */
+/* Deterministic initial conditions in the field order above; call with
+   fields == NULL to get the particle count.  Evrard sphere:
+   Solver::make_evrard (src/sample/evrard.cpp:13-87). */
+int64_t sphgpu_sample_evrard(int N, double G, double gamma, double* const* fields);
+/* 3-D periodic shear layer after Solver::make_khi (src/sample/khi.cpp:12-73). */
+int64_t sphgpu_sample_shear_layer(double dx, double lz, double gamma, double* const* fields);
+/* 3-D shock tube along x in [-0.5, 0.5] x [0, ly]^2. */
+int64_t sphgpu_sample_shock_tube(double dx, double ly, double p_left, double p_right, double gamma,
+                                 double* const* fields);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,33 @@
+"""The C++ host mirror (host/sphgpu.hpp) compiles against the C ABI and
+drives the modules like the reference's Solver."""
+import os
+import subprocess
+
+import pytest
+
+from conftest import PKG, ROOT
+
+
+def _build(tmp_path):
+    exe = tmp_path / "host_mirror"
+    cmd = ["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"), "-I", os.path.join(PKG, "host"),
+           os.path.join(ROOT, "tests", "cpp", "host_mirror.cpp"), "-L", PKG, "-lsphgpu", f"-Wl,-rpath,{PKG}",
+           "-o", str(exe)]
+    subprocess.run(cmd, check=True, capture_output=True)
+    return exe
+
+
+def test_host_mirror_compiles_and_fails_loudly_without_device(G, tmp_path):
+    exe = _build(tmp_path)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    if G.device_ok():
+        pytest.skip("a device is present (covered by the gpu test)")
+    assert r.returncode == 3, r.stdout + r.stderr
+
+
+@pytest.mark.gpu
+def test_host_mirror_runs_steps(gpu, tmp_path):
+    exe = _build(tmp_path)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "neighbours(0)=" in r.stdout
