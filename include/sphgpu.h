@@ -233,6 +233,27 @@ int sphgpu_timer_stop(sphgpu_ctx* ctx, double* ms);
 /* Kernels this context launched since timing was last enabled. */
 int64_t sphgpu_launch_count(const sphgpu_ctx* ctx);
 
+/* ---------------- allocation-free entry point ---------------- */
+/* No counterpart in the reference.  TimeStep::calculation for callers that
+   cannot allocate device memory when they need dt (e.g. a host solver whose
+   device memory is entirely owned by its own pool, or code that must not
+   incur the synchronisation of cudaMalloc/cudaFree).  Inputs and the result
+   are caller-owned DEVICE memory: acc_xyz = 3n doubles (x, y, z per
+   particle), sml = n doubles, dt_out = 1 double; stream = cudaStream_t
+   (NULL = default stream).  Nothing is allocated: the reduction scratch is a
+   fixed file-scope device array of SPHGPU_NOALLOC_MAX_BLOCKS doubles that
+   every GPU loading the library keeps until exit.  n above
+   SPHGPU_NOALLOC_MAX_PARTICLES is rejected with SPHGPU_ERR_ARG.  The first
+   call on a device looks up the array's device address (make it before any
+   stream capture).  All calls share the array: calls that overlap on the GPU
+   race. */
+#define SPHGPU_NOALLOC_TILE 1024
+#define SPHGPU_NOALLOC_MAX_BLOCKS 4096
+#define SPHGPU_NOALLOC_MAX_PARTICLES (SPHGPU_NOALLOC_TILE * SPHGPU_NOALLOC_MAX_BLOCKS)
+int sphgpu_timestep_noalloc(const double* acc_xyz, const double* sml, int64_t n,
+                            double h_per_v_sig, double cfl_sound, double cfl_force,
+                            double* dt_out, void* stream);
+
 /* ---------------- learned Riemann guess (no reference counterpart) ------ */
 /* The MLP maps (log rho_R/rho_L, log p_R/p_L, (u_R-u_L)/c_L, c_R/c_L, gamma)
    to log(p_star / p_L) through 3 hidden layers of 64 SiLU units. Weights are BF16
