@@ -208,6 +208,11 @@ int sphgpu_integrate(sphgpu_ctx* ctx);
 int sphgpu_energies(sphgpu_ctx* ctx, double* kinetic, double* thermal,
                     double* potential, double* mom);
 
+/* Neighbour-walk implementation: 0 (default) = warp-level group walk with
+   exact fallback for pairs on the search radius; 1 = per-lane walk that
+   replays the reference's recursion test by test.  Both give the same sets;
+   mode 1 exists for cross-checking. */
+int sphgpu_set_walk_mode(sphgpu_ctx* ctx, int mode);
 /* PreInteraction::m_first (src/pre_interaction.cpp:41-44): whether the next
    PreInteraction call runs initial_smoothing first.  Set after upload; turn
    it off to continue from a state whose density is already an SPH density

@@ -167,6 +167,7 @@ int alloc_all(sphgpu_ctx* c, int n)
     const int nc = c->node_cap;
     if((rc = dalloc(c, c->t.geo, nc)) || (rc = dalloc(c, c->t.mass, nc)) || (rc = dalloc(c, c->t.ksize, nc))
        || (rc = dalloc(c, c->t.link, nc)) || (rc = dalloc(c, c->t.parent, nc)) || (rc = dalloc(c, c->t.nchild, nc))
+       || (rc = dalloc(c, c->t.child, 8 * (size_t)nc))
        || (rc = dalloc(c, c->t.counter, nc)) || (rc = dalloc(c, c->t.nnodes, 4)))
         return rc;
     if((rc = dalloc(c, c->d_root, 1)) || (rc = dalloc(c, c->d_bbox_part, 6 * 1024)) || (rc = dalloc(c, c->d_keys, n))
@@ -606,6 +607,13 @@ int sphgpu_energies(sphgpu_ctx* c, double* K, double* U, double* W, double* mom)
         mom[1] = out[4];
         mom[2] = out[5];
     }
+    return SPHGPU_OK;
+}
+
+int sphgpu_set_walk_mode(sphgpu_ctx* c, int mode)
+{
+    if(!c || mode < 0 || mode > 1) return SPHGPU_ERR_ARG;
+    c->walk_mode = mode;
     return SPHGPU_OK;
 }
 

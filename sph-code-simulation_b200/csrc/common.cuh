@@ -62,6 +62,7 @@ struct DevTree {
     double4* mass;   // centre of mass x, y, z, mass
     double* ksize;   // kernel_size: max sml in the subtree
     int4* link;      // start, end, skip, level | is_leaf << 8
+    int* child;      // 8 slots per node (child index by octant, -1 = none)
     int* parent;
     int* nchild;
     int* counter;

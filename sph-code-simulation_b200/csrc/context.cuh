@@ -63,6 +63,8 @@ struct sphgpu_ctx {
 
     // counters kept on the host
     int64_t retries = 0;
+    int64_t walk_fallbacks = 0;     // group walks redone by the per-lane walk
+    int walk_mode = 0;              // 0 = group walk, 1 = per-lane walk only
     int64_t max_gather = 0, max_pair = 0, node_count = 0;
 
     // timing: event pairs recorded around each stage and read back at the

@@ -276,6 +276,8 @@ __global__ void k_nodes(const uint64_t* __restrict__ keys, int n, int D, const i
         }
         T.parent[idx] = par;
         atomicAdd(&T.nchild[par], 1);
+        // octant of this node in its parent = the key digit taken at level L-1
+        T.child[(size_t)par * 8 + (int)((kp >> (3 * (D - (L - 1)))) & 7)] = idx;
         if(L < leaf) {
             const int d = (int)((kp >> (3 * (D - L))) & 7);
             cx = child_center(cx, d & 1, e);
@@ -456,6 +458,7 @@ int tree_make(sphgpu_ctx* c)
     k_levels<<<grid_for(n, BLK), BLK, 0, st>>>(c->d_keys, n, D, c->prm.leaf_particle_num, c->d_nstart, c->d_lvl);
     launches += exclusive_scan(c->d_nstart, c->d_base, n, (int*)nullptr, c->scan, st);
     SPHGPU_CUDA(c, cudaMemsetAsync(c->t.nchild, 0, sizeof(int) * (size_t)c->node_cap, st));
+    SPHGPU_CUDA(c, cudaMemsetAsync(c->t.child, 0xff, sizeof(int) * 8 * (size_t)c->node_cap, st));
     k_nodes<<<grid_for(n, BLK), BLK, 0, st>>>(c->d_keys, n, D, c->d_nstart, c->d_base, c->d_lvl, c->d_root,
                                               c->node_cap, c->t, c->d_leaf_of_start, c->d_status);
     SPHGPU_LAUNCH_CHECK(c, "tree_make: node pass");

@@ -112,6 +112,234 @@ __global__ void __launch_bounds__(WBLK) k_walk(DevParams P, DevState S, DevTree 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Group walk.  The set a particle i gets from the reference's recursion is
+//   { j : r_ij^2 < h^2  and every box test on the path root -> leaf(j) passes }
+// with h = sml_i (gather) or max(sml_i, kernel_size) per node (is_ij).  A box
+// test compares the L-infinity distance from x_i to the node centre with
+// edge/2 + h.  Particle j lies inside every ancestor's box up to the rounding
+// of the node centres (<= ~20 ulp of the coordinate scale), and the test
+// radius only grows towards the root, so when r_ij < h_leaf - delta (delta =
+// 1e-12 of the domain scale, thousands of ulp) every test on the path passes.
+// Only pairs with h_leaf - delta <= r_ij < h_leaf need the reference's tests,
+// which are then replayed exactly up the parent chain.
+//
+// Traversal is therefore done once per warp for the group's bounding box:
+// each step the 32 lanes test 32 stack nodes in parallel (a conservative
+// superset test), push the children of passing internal nodes (LIFO stack in
+// shared memory) and queue passing leaves; queued leaves are tested in
+// batches, each lane against its own particle.  A stack overflow marks the
+// warp and the host re-runs the call with the per-lane walk.
+constexpr int GW_WARPS = 4;
+constexpr int GW_STACK = 1024;
+constexpr int GW_QUEUE = 64;
+
+__device__ __forceinline__ double interval_gap(double c, double lo, double hi)
+{
+    return c < lo ? lo - c : (c > hi ? c - hi : 0.0);
+}
+
+// exact box test of the reference's recursion at node nd for particle i
+template <bool IJ>
+__device__ __forceinline__ bool box_pass(const DevParams& P, const DevTree& T, int nd, double xi, double yi, double zi,
+                                         double hi)
+{
+    const double4 g = ldg4(&T.geo[nd]);
+    double h = hi;
+    if(IJ) {
+        const double ks = __ldg(&T.ksize[nd]);
+        h = hi < ks ? ks : hi;
+    }
+    const double l2 = (g.w * 0.5 + h) * (g.w * 0.5 + h);
+    const Vec3d d = rij(P, xi, yi, zi, g.x, g.y, g.z);
+    double m = d.x * d.x;
+    const double m1 = d.y * d.y, m2 = d.z * d.z;
+    if(m1 > m) m = m1;
+    if(m2 > m) m = m2;
+    return m <= l2;
+}
+
+template <bool IJ>
+__global__ void __launch_bounds__(GW_WARPS * 32) k_walk_group(DevParams P, DevState S, DevTree T, int n, int cap,
+                                                             int* __restrict__ list, int* __restrict__ count,
+                                                             DevStatus* __restrict__ st, int guess, double ratio)
+{
+    __shared__ int s_stack[GW_WARPS][GW_STACK];
+    __shared__ int s_queue[GW_WARPS][GW_QUEUE];
+    __shared__ double4 s_cpos[GW_WARPS][32];
+    __shared__ int4 s_clink[GW_WARPS][32];
+    __shared__ double s_cks[GW_WARPS][32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * GW_WARPS + w) * 32 + lane;
+    const bool valid = i < n;
+    if(__ballot_sync(FULL_MASK, valid) == 0) return;  // whole warp past the end
+    double xi = 0, yi = 0, zi = 0, hi = 0;
+    if(valid) {
+        const double4 p = S.pos[i];
+        xi = p.x;
+        yi = p.y;
+        zi = p.z;
+        if(guess) {
+            constexpr double A = 4.0 * 3.14159265358979323846 / 3.0;
+            hi = pow(P.nngb * p.w / (S.thermo[i].x * A), 1.0 / 3) * ratio;
+            S.vel[i].w = hi;
+        } else {
+            hi = S.vel[i].w;
+        }
+    }
+    // group bounding box and largest radius
+    double lo[3] = {valid ? xi : 1e300, valid ? yi : 1e300, valid ? zi : 1e300};
+    double up[3] = {valid ? xi : -1e300, valid ? yi : -1e300, valid ? zi : -1e300};
+    double hmax = valid ? hi : 0.0;
+    for(int o = 16; o > 0; o >>= 1) {
+        for(int k = 0; k < 3; ++k) {
+            lo[k] = fmin(lo[k], __shfl_xor_sync(FULL_MASK, lo[k], o));
+            up[k] = fmax(up[k], __shfl_xor_sync(FULL_MASK, up[k], o));
+        }
+        hmax = fmax(hmax, __shfl_xor_sync(FULL_MASK, hmax, o));
+    }
+    // safety margin for the fast acceptance (see above)
+    const double4 root = ldg4(&T.geo[0]);
+    const double scale = fmax(fabs(root.x), fmax(fabs(root.y), fabs(root.z))) + root.w;
+    const double delta = 1e-12 * scale;
+
+    const size_t row = (size_t)(valid ? i : 0) * (size_t)cap;
+    int cnt = 0;
+    int sp = 0, nq = 0;
+    bool overflow = false;
+    if(lane == 0) s_stack[w][0] = 0;
+    sp = 1;
+    __syncwarp();
+
+    auto process = [&](int nproc) {
+        // lanes load one queued leaf each, then every lane tests all of them
+        const int L = lane < nproc ? s_queue[w][lane] : -1;
+        if(L >= 0) {
+            const int4 lk = __ldg(&T.link[L]);
+            s_clink[w][lane] = make_int4(lk.x, lk.y, L, 0);
+            s_cpos[w][lane] = ldg4(&S.pos[lk.x]);
+            s_cks[w][lane] = IJ ? __ldg(&T.ksize[L]) : 0.0;
+        }
+        __syncwarp();
+        if(valid) {
+            for(int t = 0; t < nproc; ++t) {
+                const int4 cl = s_clink[w][t];
+                double h = hi;
+                if(IJ) {
+                    const double ks = s_cks[w][t];
+                    h = hi < ks ? ks : hi;
+                }
+                const double h2 = h * h;
+                const double hs = h - delta;
+                const double hs2 = hs > 0.0 ? hs * hs : -1.0;
+                for(int q = cl.x; q < cl.y; ++q) {
+                    const double4 pj = q == cl.x ? s_cpos[w][t] : ldg4(&S.pos[q]);
+                    const Vec3d r = rij(P, xi, yi, zi, pj.x, pj.y, pj.z);
+                    const double r2 = abs2x(r);
+                    if(!(r2 < h2)) continue;
+                    bool take = r2 < hs2;
+                    if(!take) {
+                        // on the radius: replay the reference's box tests up the path
+                        take = true;
+                        int A = cl.z;
+                        for(int up_ = 0; A >= 0 && up_ < 64; ++up_) {
+                            if(!box_pass<IJ>(P, T, A, xi, yi, zi, hi)) {
+                                take = false;
+                                break;
+                            }
+                            A = A == 0 ? -1 : T.parent[A];
+                        }
+                    }
+                    if(take) {
+                        if(cnt < cap) list[row + cnt] = q;
+                        ++cnt;
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    };
+
+    const int nnodes = *T.nnodes;
+    int steps = 0;
+    while(sp > 0) {
+        if(++steps > nnodes + 1) {  // each node is pushed at most once
+            overflow = true;
+            break;
+        }
+        const int m = sp < 32 ? sp : 32;
+        const int nd = lane < m ? s_stack[w][sp - 1 - lane] : -1;
+        __syncwarp();
+        sp -= m;
+        bool pass = false, leaf = false;
+        int4 c0 = make_int4(-1, -1, -1, -1), c1 = c0;
+        if(nd >= 0) {
+            const int4 lk = __ldg(&T.link[nd]);
+            const double4 g = ldg4(&T.geo[nd]);
+            leaf = (lk.w >> 8) != 0;
+            double hh = hmax;
+            if(IJ) hh = fmax(hmax, __ldg(&T.ksize[nd]));
+            const double reach = (g.w * 0.5 + hh) * (1.0 + 1e-10) + delta;
+            const double cc[3] = {g.x, g.y, g.z};
+            pass = true;
+            for(int k = 0; k < 3; ++k) {
+                double gap = interval_gap(cc[k], lo[k], up[k]);
+                if(P.periodic) {
+                    gap = fmin(gap, interval_gap(cc[k] + P.range[k], lo[k], up[k]));
+                    gap = fmin(gap, interval_gap(cc[k] - P.range[k], lo[k], up[k]));
+                }
+                pass = pass && gap <= reach;
+            }
+            if(pass && !leaf) {
+                const int4* cp = reinterpret_cast<const int4*>(T.child + (size_t)nd * 8);
+                c0 = __ldg(cp);
+                c1 = __ldg(cp + 1);
+            }
+        }
+        // push children of passing internal nodes (order within a step is free)
+        const int kids[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+        int nk = 0;
+        for(int k = 0; k < 8; ++k) nk += kids[k] >= 0 ? 1 : 0;
+        int incl = nk;
+        for(int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(FULL_MASK, incl, o);
+            if(lane >= o) incl += u;
+        }
+        const int total = __shfl_sync(FULL_MASK, incl, 31);
+        if(sp + total > GW_STACK) {
+            overflow = true;
+            break;
+        }
+        int pos = sp + incl - nk;
+        for(int k = 0; k < 8; ++k) {
+            if(kids[k] >= 0) s_stack[w][pos++] = kids[k];
+        }
+        sp += total;
+        // queue passing leaves
+        const unsigned lb = __ballot_sync(FULL_MASK, pass && leaf);
+        if(pass && leaf) s_queue[w][nq + __popc(lb & ((1u << lane) - 1u))] = nd;
+        nq += __popc(lb);
+        __syncwarp();
+        if(nq >= 32) {
+            process(32);
+            nq -= 32;
+            if(lane < nq) s_queue[w][lane] = s_queue[w][32 + lane];
+            __syncwarp();
+        }
+    }
+    if(!overflow && nq > 0) process(nq);
+    if(overflow) {
+        if(lane == 0) st->guard = 2;
+        return;
+    }
+    if(valid) {
+        count[i] = cnt;
+        if(cnt > cap) st->overflow = 1;
+        if(cnt > P.nngb * 1000) st->fatal = 1;
+        atomicMax(&st->max_count, cnt);
+    }
+}
+
 // exhaustive_search (src/exhaustive_search.cpp:11-42): all j with
 // r^2 < h_i^2 (gather) or r^2 < max(h_i^2, h_j^2) (is_ij).
 __global__ void k_exhaustive(DevParams P, DevState S, int n, int is_ij, int cap, int* __restrict__ list,
@@ -166,7 +394,8 @@ int run_walk(sphgpu_ctx* c, int which, bool guess, double ratio, bool exhaustive
 {
     cudaStream_t st = c->stream;
     const int n = c->n;
-    for(int attempt = 0; attempt < 4; ++attempt) {
+    bool per_lane = false;
+    for(int attempt = 0; attempt < 6; ++attempt) {
         ++*launches;
         const int64_t cap = which == 0 ? c->gcap : c->pcap;
         int* list = which == 0 ? c->d_glist : c->d_plist;
@@ -175,6 +404,15 @@ int run_walk(sphgpu_ctx* c, int which, bool guess, double ratio, bool exhaustive
         SPHGPU_CUDA(c, cudaMemsetAsync(&c->d_status->guard, 0, sizeof(int), st));
         if(exhaustive) {
             k_exhaustive<<<grid_for(n, 128), 128, 0, st>>>(c->dp, c->s, n, is_ij, (int)cap, list, count, c->d_status);
+        } else if(c->walk_mode == 0 && !per_lane) {
+            const unsigned grid = grid_for(n, GW_WARPS * 32);
+            if(which == 0) {
+                k_walk_group<false><<<grid, GW_WARPS * 32, 0, st>>>(c->dp, c->s, c->t, n, (int)cap, list, count,
+                                                                   c->d_status, guess ? 1 : 0, ratio);
+            } else {
+                k_walk_group<true><<<grid, GW_WARPS * 32, 0, st>>>(c->dp, c->s, c->t, n, (int)cap, list, count,
+                                                                  c->d_status, 0, 1.0);
+            }
         } else if(which == 0) {
             k_walk<false><<<grid_for(n, WBLK), WBLK, 0, st>>>(c->dp, c->s, c->t, n, (int)cap, list, count,
                                                             c->d_status, guess ? 1 : 0, ratio);
@@ -188,6 +426,12 @@ int run_walk(sphgpu_ctx* c, int which, bool guess, double ratio, bool exhaustive
         if(c->h_status.fatal) {
             return fail(c, SPHGPU_ERR_NEIGHBOR_OVERFLOW,
                         "Neighbor list overflow: more than neighborNumber * 1000 neighbours");
+        }
+        if(c->h_status.guard == 2 && !per_lane) {
+            // a warp's traversal stack overflowed: redo this call with the per-lane walk
+            per_lane = true;
+            ++c->walk_fallbacks;
+            continue;
         }
         if(c->h_status.guard) return fail(c, SPHGPU_ERR_STATE, "tree walk exceeded the node count (corrupt tree)");
         if(which == 0) c->max_gather = c->h_status.max_count;

@@ -129,6 +129,7 @@ def lib() -> C.CDLL:
         "sphgpu_get_stage_times": (C.c_int, [vp, dp, i64p]),
         "sphgpu_synchronize": (C.c_int, [vp]),
         "sphgpu_set_initial_smoothing": (C.c_int, [vp, C.c_int]),
+        "sphgpu_set_walk_mode": (C.c_int, [vp, C.c_int]),
         "sphgpu_timer_start": (C.c_int, [vp]),
         "sphgpu_timer_stop": (C.c_int, [vp, dp]),
         "sphgpu_launch_count": (i64, [vp]),
@@ -325,6 +326,10 @@ class Simulation:
         self._check(lib().sphgpu_energies(self._h, C.byref(k), C.byref(u), C.byref(w),
                                           C.cast(mom, C.POINTER(C.c_double))), "energies")
         return k.value, u.value, w.value, np.array(mom[:])
+
+    def set_walk_mode(self, mode: int):
+        """0 = group walk (default), 1 = per-lane walk (cross-check)."""
+        self._check(lib().sphgpu_set_walk_mode(self._h, int(mode)), "set_walk_mode")
 
     def set_initial_smoothing(self, on: bool):
         self._check(lib().sphgpu_set_initial_smoothing(self._h, int(on)), "set_initial_smoothing")
