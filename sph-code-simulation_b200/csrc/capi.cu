@@ -674,6 +674,9 @@ int sphgpu_get_counters(sphgpu_ctx* c, sphgpu_counters* o)
     o->max_pair = c->max_pair;
     o->node_count = c->node_count;
     o->retries = c->retries;
+    o->walk_group_warps = (int64_t)c->h_status.walk_group_warps;
+    o->walk_lane_warps = (int64_t)c->h_status.walk_lane_warps;
+    o->walk_fallbacks = c->walk_fallbacks;
     return SPHGPU_OK;
 }
 

@@ -80,6 +80,8 @@ struct DevStatus {
     unsigned long long riemann_solves;
     unsigned long long riemann_iters;
     unsigned long long riemann_fallbacks;
+    unsigned long long walk_group_warps;   // warps that took the group walk
+    unsigned long long walk_lane_warps;    // warps that took the per-lane walk
 };
 
 // Read-only 32-byte load through the non-coherent path (two 16-byte halves).
@@ -99,9 +101,13 @@ __device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a,
 __device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
 
 // Periodic::calc_r_ij (include/periodic.hpp:34-59), one axis: candidates
-// d, d + L, d - L with the first minimal |.| winning ties.
+// d, d + L, d - L with the first minimal |.| winning ties.  Fast path: for
+// |d| <= L/2 the reference always keeps d (|d + L| and |d - L| are then
+// >= L/2 >= |d|, and a tie keeps the first candidate), so the other two
+// candidates need not be formed.
 __device__ __forceinline__ double min_image(double d, double L)
 {
+    if(fabs(d) <= 0.5 * L) return d;
     const double b = xadd(d, L), c = xsub(d, L);
     const double ad = fabs(d), ab = fabs(b), ac = fabs(c);
     if(ad <= ab && ad <= ac) return d;
@@ -192,6 +198,75 @@ struct Kern {
         const T a = T(0.5) * (fabs(T(2) - q) + T(2) - q);
         const T b = T(0.5) * (fabs(T(1) - q) + T(1) - q);
         return T(0.5) * sigma / (cube(hh) * hh) * (a * a * (T(1.5) * q - T(1.5)) + b * b * (T(-6) * q + T(3)));
+    }
+};
+
+// The same kernels with the h-dependent factors hoisted out of the pair loop
+// (one set per smoothing length): the pair then costs multiplications only,
+// plus 1/r for the cubic gradient.  Results differ from Kern<T> by rounding.
+template <typename T>
+struct KernH {
+    T inv;   // 1/h (Wendland) or 1/(h/2) (cubic)
+    T wn;    // W = wn * shape(q)
+    T dwn;   // grad W = r_ij * dwn * shape'(q)  (cubic: times 1/r)
+    T dhn;   // dW/dh = dhn * shape_h(q)
+    int type;
+
+    __device__ __forceinline__ KernH(int type_, T h) : type(type_)
+    {
+        constexpr double PI = 3.14159265358979323846;
+        if(type == SPHGPU_WENDLAND) {
+            const T sigma = T(495.0 / (32.0 * PI));
+            inv = T(1) / h;
+            const T i3 = inv * inv * inv;
+            wn = sigma * i3;
+            dwn = T(-56.0 / 3.0) * sigma * i3 * inv * inv;
+            dhn = -sigma * i3 * inv * T(1.0 / 3.0);
+        } else {
+            const T sigma = T(1.0 / PI);
+            inv = T(2) / h;
+            const T i3 = inv * inv * inv;
+            wn = sigma * i3;
+            dwn = -sigma * i3 * inv;
+            dhn = T(0.5) * sigma * i3 * inv;
+        }
+    }
+    __device__ __forceinline__ T w(T r) const
+    {
+        const T q = r * inv;
+        if(type == SPHGPU_WENDLAND) {
+            const T a = T(0.5) * (T(1) - q + fabs(T(1) - q));
+            const T a2 = a * a;
+            return wn * (a2 * a2 * a2) * (T(1) + T(6) * q + T(35.0 / 3.0) * q * q);
+        }
+        const T a = T(0.5) * (T(2) - q + fabs(T(2) - q));
+        const T b = T(0.5) * (T(1) - q + fabs(T(1) - q));
+        return wn * (T(0.25) * a * a * a - b * b * b);
+    }
+    __device__ __forceinline__ T dwc(T r, T rinv) const
+    {
+        const T q = r * inv;
+        if(type == SPHGPU_WENDLAND) {
+            const T a = T(0.5) * (T(1) - q + fabs(T(1) - q));
+            const T a2 = a * a;
+            return dwn * (a2 * a2 * a) * (T(1) + T(5) * q);
+        }
+        if(r == T(0)) return T(0);
+        const T a = T(0.5) * (T(2) - q + fabs(T(2) - q));
+        const T b = T(0.5) * (T(1) - q + fabs(T(1) - q));
+        return dwn * rinv * (T(0.75) * a * a - T(3) * b * b);
+    }
+    __device__ __forceinline__ T dhw(T r) const
+    {
+        const T q = r * inv;
+        if(type == SPHGPU_WENDLAND) {
+            const T a = T(0.5) * (T(1) - q + fabs(T(1) - q));
+            const T a2 = a * a;
+            return dhn * (a2 * a2 * a) * (T(9) + T(45) * q + T(-5) * q * q - T(385) * q * q * q);
+        }
+        const T a = T(0.5) * (T(2) - q + fabs(T(2) - q));
+        const T b = T(0.5) * (T(1) - q + fabs(T(1) - q));
+        return dhn * (a * a * (T(1.5) * q - T(1.5)) + b * b * (T(-6) * q + T(3)));
     }
 };
 

@@ -194,6 +194,13 @@ __global__ void __launch_bounds__(FBLK) k_force(DevParams P, DevState S, int n, 
         }
         const T rhoi = (T)ti.x, Pi = (T)ti.y, ui = (T)ti.z, ci = (T)ti.w;
         const T mi = (T)pi.w;
+        const KernH<T> khi(P.kernel, (T)hi);
+        // per-particle factors of the pair terms
+        const T ppr = Pi / (rhoi * rhoi);                             // ssph P_i / rho_i^2
+        const T g2u = ((T)gamma - T(1)) * ((T)gamma - T(1)) * ui;     // disph (gamma-1)^2 u_i
+        const T g2up = g2u / Pi;
+        const T mu_inv = T(1) / (mi * ui);
+        const T r2i = T(1) / (rhoi * rhoi);
         double ax = 0, ay = 0, az = 0, de = 0;
         for(int k = lane; k < cnt; k += G) {
             const int j = li[k];
@@ -205,9 +212,11 @@ __global__ void __launch_bounds__(FBLK) k_force(DevParams P, DevState S, int n, 
             if(r >= (hi < hj ? hj : hi) || r == 0.0) continue;
             const double4 tj = S.thermo[j];
             const T rT = (T)r;
+            const T rinvT = (T)(1.0 / r);
             const V3<T> rv{(T)d.x, (T)d.y, (T)d.z};
-            const T ci_ = Kern<T>::dwc(P.kernel, rT, (T)hi);
-            const T cj_ = Kern<T>::dwc(P.kernel, rT, (T)hj);
+            const KernH<T> khj(P.kernel, (T)hj);
+            const T ci_ = khi.dwc(rT, rinvT);
+            const T cj_ = khj.dwc(rT, rinvT);
             const V3<T> dwi{rv.x * ci_, rv.y * ci_, rv.z * ci_};
             const V3<T> dwj{rv.x * cj_, rv.y * cj_, rv.z * cj_};
             const T mj = (T)pj.w;
@@ -280,7 +289,7 @@ __global__ void __launch_bounds__(FBLK) k_force(DevParams P, DevState S, int n, 
                 }
                 // f = dw_i m_j p* / rho_i^2 + dw_j m_j p* / rho_j^2 (src/gsph/g_fluid_force.cpp:158-165)
                 const T ps = (T)pstar;
-                const T fi = mj * ps * (T(1) / (rhoi * rhoi));
+                const T fi = mj * ps * r2i;
                 const T fj = mj * ps * (T(1) / (rhoj * rhoj));
                 const double fx = (double)(dwi.x * fi + dwj.x * fj);
                 const double fy = (double)(dwi.y * fi + dwj.y * fj);
@@ -300,7 +309,7 @@ __global__ void __launch_bounds__(FBLK) k_force(DevParams P, DevState S, int n, 
             if(vr < T(0)) {
                 const T alpha = T(0.5) * ((T)si.x + (T)sj.x);
                 const T bal = T(0.5) * ((T)si.y + (T)sj.y);
-                const T w = vr / rT;
+                const T w = vr * rinvT;
                 const T vsig = ci + cj - T(3) * w;
                 const T rinv = T(2) / (rhoi + rhoj);
                 pij = -T(0.5) * bal * alpha * vsig * w * rinv;
@@ -308,22 +317,19 @@ __global__ void __launch_bounds__(FBLK) k_force(DevParams P, DevState S, int n, 
             // artificial conductivity (src/fluid_force.cpp:108-116)
             T dac = 0;
             if(P.use_ac) {
-                const T vs = P.gravity ? fabs(vr / rT) : sqrt(T(2) * fabs(Pi - Pj) / (rhoi + rhoj));
-                dac = (T)P.alpha_ac * mj * vs * (ui - uj) * (dwij.x * rv.x + dwij.y * rv.y + dwij.z * rv.z) / rT;
+                const T vs = P.gravity ? fabs(vr * rinvT) : sqrt(T(2) * fabs(Pi - Pj) / (rhoi + rhoj));
+                dac = (T)P.alpha_ac * mj * vs * (ui - uj) * (dwij.x * rv.x + dwij.y * rv.y + dwij.z * rv.z) * rinvT;
             }
             const T vdwi = vij.x * dwi.x + vij.y * dwi.y + vij.z * dwi.z;
             const T vdwij = vij.x * dwij.x + vij.y * dwij.y + vij.z * dwij.z;
             T a_i, a_j, e_;
             if(TYPE == SPHGPU_DISPH) {
-                const T g2u = ((T)gamma - T(1)) * ((T)gamma - T(1)) * ui;
-                const T g2up = g2u / Pi;
                 const T fij = T(1) - (T)si.z / (mj * uj);
-                const T fji = T(1) - (T)sj.z / (mi * ui);
+                const T fji = T(1) - (T)sj.z * mu_inv;
                 a_i = mj * (g2up * uj * fij + T(0.5) * pij);
                 a_j = mj * (g2u * (uj / Pj) * fji + T(0.5) * pij);
                 e_ = mj * g2up * uj * fij * vdwi + T(0.5) * mj * pij * vdwij + dac;
             } else {
-                const T ppr = Pi / (rhoi * rhoi);
                 a_i = mj * (ppr * (T)si.z + T(0.5) * pij);
                 a_j = mj * (Pj / (rhoj * rhoj) * (T)sj.z + T(0.5) * pij);
                 e_ = mj * ppr * (T)si.z * vdwi + T(0.5) * mj * pij * vdwij + dac;

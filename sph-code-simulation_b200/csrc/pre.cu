@@ -73,13 +73,14 @@ __global__ void __launch_bounds__(PBLK) k_pre(DevParams P, DevState S, int n, co
             for(int it = 0; it < 10; ++it) {
                 const double hb = h;
                 T d = 0, dd = 0;
+                const KernH<T> kh(P.kernel, (T)h);
                 for(int k = lane; k < cnt; k += G) {
                     const double4 pj = S.pos[li[k]];
                     Vec3d dv;
                     const double r = exact_r(P, pi.x, pi.y, pi.z, pj, dv);
                     if(r < h) {
-                        const T w = Kern<T>::w(P.kernel, (T)r, (T)h);
-                        const T dh = Kern<T>::dhw(P.kernel, (T)r, (T)h);
+                        const T w = kh.w((T)r);
+                        const T dh = kh.dhw((T)r);
                         if(disph) {
                             d += w;
                             dd += dh;
@@ -106,7 +107,7 @@ __global__ void __launch_bounds__(PBLK) k_pre(DevParams P, DevState S, int n, co
         }
 
         // ---- 2. fused pass over {r < h}
-        const T hT = (T)h;
+        const KernH<T> kh(P.kernel, (T)h);
         T dens = 0, dhd = 0, ni = 0, pres = 0, dhp = 0, dhn = 0;
         T divv = 0, rx = 0, ry = 0, rz = 0;
         T gd[3] = {0, 0, 0}, gu[3] = {0, 0, 0}, gv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -124,10 +125,11 @@ __global__ void __launch_bounds__(PBLK) k_pre(DevParams P, DevState S, int n, co
             const double4 vj = S.vel[j];
             const double4 tj = S.thermo[j];
             const T rT = (T)r;
-            const T w = Kern<T>::w(P.kernel, rT, hT);
+            const double rinv = r > 0.0 ? 1.0 / r : 0.0;
+            const T w = kh.w(rT);
             const T mj = (T)pj.w;
             if(disph) {
-                const T dh = Kern<T>::dhw(P.kernel, rT, hT);
+                const T dh = kh.dhw(rT);
                 const T uj = (T)tj.z;
                 dens += mj * w;
                 ni += w;
@@ -136,15 +138,15 @@ __global__ void __launch_bounds__(PBLK) k_pre(DevParams P, DevState S, int n, co
                 dhn += dh;
             } else {
                 dens += mj * w;
-                if(!gsph) dhd += mj * Kern<T>::dhw(P.kernel, rT, hT);
+                if(!gsph) dhd += mj * kh.dhw(rT);
             }
             if(i != j) {
                 const double vr = dv.x * (vi.x - vj.x) + dv.y * (vi.y - vj.y) + dv.z * (vi.z - vj.z);
-                const double v = ti.w + tj.w - 3.0 * vr / r;
+                const double v = ti.w + tj.w - 3.0 * vr * rinv;
                 if(v > vsig) vsig = v;
             }
             if(need_av || need_grad) {
-                const T c = Kern<T>::dwc(P.kernel, rT, hT);
+                const T c = kh.dwc(rT, (T)rinv);
                 const T dwx = (T)dv.x * c, dwy = (T)dv.y * c, dwz = (T)dv.z * c;
                 const T vx = (T)(vi.x - vj.x), vy = (T)(vi.y - vj.y), vz = (T)(vi.z - vj.z);
                 if(need_av) {
@@ -318,12 +320,13 @@ __global__ void __launch_bounds__(PBLK) k_initial_density(DevParams P, DevState 
         const int* li = list + (size_t)(valid ? i : 0) * (size_t)cap;
         const double4 pi = valid ? S.pos[i] : make_double4(0, 0, 0, 0);
         const double h = valid ? S.vel[i].w : 1.0;
+        const KernH<T> kh(P.kernel, (T)h);
         T d = 0;
         for(int k = lane; k < cnt; k += G) {
             const double4 pj = S.pos[li[k]];
             Vec3d dv;
             const double r = exact_r(P, pi.x, pi.y, pi.z, pj, dv);
-            if(r < h) d += (T)pj.w * Kern<T>::w(P.kernel, (T)r, (T)h);
+            if(r < h) d += (T)pj.w * kh.w((T)r);
         }
         const double ds = (double)group_sum<G>(d);
         if(valid && lane == 0) S.thermo[i].x = ds;

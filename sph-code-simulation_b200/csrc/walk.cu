@@ -30,31 +30,14 @@ namespace {
 
 constexpr int WBLK = 128;
 
+// Per-lane walk of one particle (lane) over the preorder node array; the
+// caller's warp runs it in lock step.  Returns the list length.
 template <bool IJ>
-__global__ void __launch_bounds__(WBLK) k_walk(DevParams P, DevState S, DevTree T, int n, int cap,
-                                               int* __restrict__ list, int* __restrict__ count,
-                                               DevStatus* __restrict__ st, int guess, double ratio)
+__device__ __forceinline__ int walk_lanes(const DevParams& P, const DevState& S, const DevTree& T, bool valid,
+                                          double xi, double yi, double zi, double hi, int* __restrict__ list,
+                                          size_t row, int cap, DevStatus* __restrict__ st)
 {
-    const int i = blockIdx.x * WBLK + threadIdx.x;
-    const bool valid = i < n;
-    double xi = 0, yi = 0, zi = 0, hi = 0;
-    if(valid) {
-        const double4 p = S.pos[i];
-        xi = p.x;
-        yi = p.y;
-        zi = p.z;
-        if(guess) {
-            // h guess from the previous density (src/pre_interaction.cpp:61-64)
-            constexpr double A = 4.0 * 3.14159265358979323846 / 3.0;
-            const double dens = S.thermo[i].x;
-            hi = pow(P.nngb * p.w / (dens * A), 1.0 / 3) * ratio;
-            S.vel[i].w = hi;
-        } else {
-            hi = S.vel[i].w;
-        }
-    }
     const int nnodes = *T.nnodes;
-    const size_t row = (size_t)i * (size_t)cap;
     int cnt = 0;
     unsigned bits = 0;
     int nd = 0, steps = 0;
@@ -104,6 +87,34 @@ __global__ void __launch_bounds__(WBLK) k_walk(DevParams P, DevState S, DevTree 
             nd = __any_sync(FULL_MASK, pass) ? nd + 1 : lk.z;
         }
     }
+    return cnt;
+}
+
+template <bool IJ>
+__global__ void __launch_bounds__(WBLK) k_walk(DevParams P, DevState S, DevTree T, int n, int cap,
+                                               int* __restrict__ list, int* __restrict__ count,
+                                               DevStatus* __restrict__ st, int guess, double ratio)
+{
+    const int i = blockIdx.x * WBLK + threadIdx.x;
+    const bool valid = i < n;
+    double xi = 0, yi = 0, zi = 0, hi = 0;
+    if(valid) {
+        const double4 p = S.pos[i];
+        xi = p.x;
+        yi = p.y;
+        zi = p.z;
+        if(guess) {
+            // h guess from the previous density (src/pre_interaction.cpp:61-64)
+            constexpr double A = 4.0 * 3.14159265358979323846 / 3.0;
+            const double dens = S.thermo[i].x;
+            hi = pow(P.nngb * p.w / (dens * A), 1.0 / 3) * ratio;
+            S.vel[i].w = hi;
+        } else {
+            hi = S.vel[i].w;
+        }
+    }
+    const size_t row = (size_t)(valid ? i : 0) * (size_t)cap;
+    const int cnt = walk_lanes<IJ>(P, S, T, valid, xi, yi, zi, hi, list, row, cap, st);
     if(valid) {
         count[i] = cnt;
         if(cnt > cap) st->overflow = 1;
@@ -198,6 +209,23 @@ __global__ void __launch_bounds__(GW_WARPS * 32) k_walk_group(DevParams P, DevSt
         }
         hmax = fmax(hmax, __shfl_xor_sync(FULL_MASK, hmax, o));
     }
+    // A window of 32 octree-ordered particles that straddles a large octant
+    // boundary has a bounding box far wider than its particles' search
+    // spheres; such warps walk per lane instead.
+    const double extent = fmax(up[0] - lo[0], fmax(up[1] - lo[1], up[2] - lo[2]));
+    if(!(extent <= 4.0 * hmax)) {
+        const size_t row0 = (size_t)(valid ? i : 0) * (size_t)cap;
+        const int c0 = walk_lanes<IJ>(P, S, T, valid, xi, yi, zi, hi, list, row0, cap, st);
+        if(lane == 0) atomicAdd(&st->walk_lane_warps, 1ull);
+        if(valid) {
+            count[i] = c0;
+            if(c0 > cap) st->overflow = 1;
+            if(c0 > P.nngb * 1000) st->fatal = 1;
+            atomicMax(&st->max_count, c0);
+        }
+        return;
+    }
+    if(lane == 0) atomicAdd(&st->walk_group_warps, 1ull);
     // safety margin for the fast acceptance (see above)
     const double4 root = ldg4(&T.geo[0]);
     const double scale = fmax(fabs(root.x), fmax(fabs(root.y), fabs(root.z))) + root.w;

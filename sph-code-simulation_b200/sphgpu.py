@@ -81,7 +81,8 @@ class Params(C.Structure):
 class Counters(C.Structure):
     _fields_ = [(n, C.c_int64) for n in (
         "newton_nonconverged", "riemann_solves", "riemann_iterations", "riemann_fallbacks",
-        "gather_capacity", "max_gather", "max_pair", "node_count", "retries")]
+        "gather_capacity", "max_gather", "max_pair", "node_count", "retries", "walk_group_warps",
+        "walk_lane_warps", "walk_fallbacks")]
 
 
 _lib = None
