@@ -35,9 +35,56 @@ import numpy as np  # noqa: E402
 
 METRIC = "particle-steps/s on 1 B200: FP64 plain vs FP32+learned-Riemann at ≤1e-5 rel err"
 UNIT = "particle-steps/s"
-WORKLOAD = "disph periodic shear layer 1.0M (Wendland C4, K=128, AC)"
-DX_1M = (0.1875 / 1.0e6) ** (1.0 / 3.0)
-DX_SAMPLE = (0.1875 / 6.5e4) ** (1.0 / 3.0)   # CPU sample of the same workload
+
+
+class Workload:
+    """One benchmark workload: parameters, initial conditions at a target size,
+    and a smaller CPU sample of the same workload for the reference arm."""
+
+    def __init__(self, name, desc, cfg, sample, default_n, cpu_n, learned=False, **overrides):
+        self.name, self.desc, self.cfg, self.sample = name, desc, cfg, sample
+        self.default_n, self.cpu_n, self.learned, self.overrides = default_n, cpu_n, learned, overrides
+
+    def params(self, G, precision):
+        p = G.config_params(self.cfg, precision=precision, **self.overrides)
+        if self.learned:
+            p.riemann_guess = G.GUESS_MLP
+        return p
+
+    def fields(self, G, n):
+        return self.sample(G, n)
+
+
+def _evrard(G, n):
+    lattice = max(8, int(round((n * 6.0 / 3.14159265) ** (1.0 / 3.0))))
+    return G.sample_evrard(lattice)
+
+
+def _shear(G, n):
+    return G.sample_shear_layer((0.1875 / n) ** (1.0 / 3.0))
+
+
+def _tube(G, n):
+    return G.sample_shock_tube((0.05 * 0.05 / n) ** (1.0 / 3.0), ly=0.05)
+
+
+WORKLOADS = {
+    "evrard_ssph": Workload("evrard_ssph", "ssph Evrard sphere 17K (cubic, K=50, leaf=1, Balsara, BH gravity)",
+                            "evrard_ssph", _evrard, 17256, 17256),
+    "shear_disph": Workload("shear_disph", "disph periodic shear layer 1.0M (Wendland C4, K=128, AC)",
+                            "shear_disph", _shear, 1.0e6, 6.5e4),
+    "tube_gsph": Workload("tube_gsph", "gsph shock tube 2.0M (MUSCL, iterative Riemann, cubic, K=50)",
+                          "tube_gsph", _tube, 2.0e6, 6.5e4),
+    "tube_gsph_mlp": Workload("tube_gsph_mlp", "gsph shock tube 2.0M with the learned Riemann guess",
+                              "tube_gsph", _tube, 2.0e6, 6.5e4, learned=True),
+    # The reference's algorithm (bit-exact oracle) turns non-finite near the
+    # sphere's centre at t ~ 0.003-0.004 on this resolution whatever the CFL;
+    # cflSound 0.05 / cflForce 0.025 keep 3 warm-up + 10 timed steps finite.
+    "evrard_disph": Workload("evrard_disph", "disph + BH gravity sphere 8.8M (Wendland C4, K=128, TD-AV, AC; "
+                             "CFL 0.05/0.025)", "evrard_disph", _evrard, 8.78e6, 6.5e4, cfl_sound=0.05,
+                             cfl_force=0.025),
+}
+DEFAULT_WORKLOAD = "shear_disph"
 
 # fields a step reads from / writes back to the caller in the e2e leg
 E2E_IN = ["pos_x", "pos_y", "pos_z", "vel_x", "vel_y", "vel_z", "acc_x", "acc_y", "acc_z", "mass", "dens",
@@ -164,37 +211,61 @@ def _pinned(n: int, names):
     return {f: torch.zeros(n, dtype=torch.float64, pin_memory=True) for f in names}
 
 
+def log(*a):
+    print("[bench]", *a, file=sys.stderr, flush=True)
+
+
 def run_gpu(args, rank: int, world: int, local: int):
     import sphgpu as G
 
     if not G.device_ok():
         raise SystemExit("bench: no usable sm_100 device")
-    fields = G.sample_shear_layer((0.1875 / args.particles) ** (1.0 / 3.0))
+    wl = WORKLOADS[args.workload]
+    fields = wl.fields(G, args.particles or wl.default_n)
     n = len(fields["pos_x"])
     hbm, peak_kind = _peaks()
 
     def timed(precision):
-        p = G.config_params("shear_disph", precision=precision)
+        log(f"{wl.name} n={n} precision={precision}: initialize")
+        p = wl.params(G, precision)
         sim = G.Simulation(p)
+        if wl.learned:
+            sim.load_riemann_mlp()
         sim.upload(fields)
         sim.initialize()
-        for _ in range(args.warmup):
+        log("warm-up")
+        for w in range(args.warmup):
             sim.integrate()
+            if args.verbose:
+                c = sim.counters()
+                log(f"warm-up step {w} done: max_gather {c['max_gather']} max_pair {c['max_pair']} "
+                    f"cap {c['gather_capacity']} retries {c['retries']} nodes {c['node_count']} "
+                    f"lane_warps {c['walk_lane_warps']} fallbacks {c['walk_fallbacks']} dt {sim.time_dt()[1]:.3e}")
         sim.synchronize()
         sim.reset_counters()
         sim.enable_timing(True)
+        log("barrier")
         barrier()
-        clocks = ClockSampler(local) if (rank == 0 and precision == G.FP64) else None
+        log("timed region")
+        clocks = ClockSampler(local) if (rank == 0 and precision == G.FP64 and not args.no_clocks) else None
         if clocks:
             clocks.start()
+        log("timer start")
         G.lib().sphgpu_timer_start(sim._h)
-        for _ in range(args.steps):
+        for k in range(args.steps):
             sim.integrate()
+            if args.verbose:
+                c = sim.counters()
+                log(f"timed step {k}: max_gather {c['max_gather']} max_pair {c['max_pair']} "
+                    f"cap {c['gather_capacity']} retries {c['retries']} nodes {c['node_count']} "
+                    f"lane_warps {c['walk_lane_warps']} fallbacks {c['walk_fallbacks']} dt {sim.time_dt()[1]:.3e}")
         import ctypes
         ms = ctypes.c_double()
         G.lib().sphgpu_timer_stop(sim._h, ctypes.byref(ms))
+        log("timer stop")
         clk = clocks.stop() if clocks else None
         barrier()
+        log(f"timed {ms.value:.1f} ms for {args.steps} steps")
         launches = int(G.lib().sphgpu_launch_count(sim._h))
         stages = sim.stage_times()
         counters = sim.counters()
@@ -256,29 +327,32 @@ def run_gpu(args, rank: int, world: int, local: int):
                  "stages_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in mstages.items()}}
         msim.close()
 
+    log("end to end")
     # end to end through the C ABI with host buffers
-    e2e = None if args.no_e2e else run_e2e(args, G, fields, world)
+    e2e = None if args.no_e2e else run_e2e(args, G, fields, world, wl)
 
     return {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if first == G.FP64 else "f32/f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD if n > 9e5 else f"{WORKLOAD} at N={n}", "n_particles": n,
+        "config": {"workload": wl.desc if not args.particles else f"{wl.desc} at N={n}", "n_particles": n,
                    "particles_per_gpu": n, "form": "fp64 plain" if first == G.FP64 else "mixed",
                    "l2": "inputs larger than L2 (state + neighbour lists ~3 GB per step)",
                    "parallelism": f"replicas x{world}"},
         "mixed": mixed, "e2e": e2e, "gpu_launches": launches,
         "stages_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in stages.items()},
-        "roofline": roofline, "clocks": clk,
+        "counters": counters, "roofline": roofline, "clocks": clk,
     }
 
 
-def run_e2e(args, G, fields, world):
+def run_e2e(args, G, fields, world, wl):
     import ctypes
     n = len(fields["pos_x"])
-    p = G.config_params("shear_disph")
+    p = wl.params(G, G.FP64)
     sim = G.Simulation(p)
+    if wl.learned:
+        sim.load_riemann_mlp()
     sim.upload(fields)
     sim.initialize()
     host_in = _pinned(n, E2E_IN)
@@ -336,13 +410,13 @@ class _QuietStdout:
         os.close(self.saved)
 
 
-def cpu_reference(steps: int, warmup: int, dx: float = DX_SAMPLE):
+def cpu_reference(steps: int, warmup: int, workload: str):
     """The reference's own OpenMP CPU build (oracle/_ref) on a bounded sample."""
     with _QuietStdout():
-        return _cpu_reference(steps, warmup, dx)
+        return _cpu_reference(steps, warmup, workload)
 
 
-def _cpu_reference(steps: int, warmup: int, dx: float):
+def _cpu_reference(steps: int, warmup: int, workload: str):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     import sphgpu as G
@@ -352,9 +426,11 @@ def _cpu_reference(steps: int, warmup: int, dx: float):
         kind, cls = "reference", O.Reference
     else:
         kind, cls = "port", O.Oracle
-    fields = G.sample_shear_layer(dx)
+    wl = WORKLOADS[workload]
+    fields = wl.fields(G, wl.cpu_n)
     n = len(fields["pos_x"])
-    p = G.config_params("shear_disph")
+    p = wl.params(G, G.FP64)
+    p.riemann_guess = G.GUESS_NONE   # the reference has no learned guess
     sim = cls(p, fields)
     sim.initialize()
     for _ in range(warmup):
@@ -373,7 +449,7 @@ def _cpu_reference(steps: int, warmup: int, dx: float):
         pass
     return {"value": n * steps / el, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": kind,
             "ms_per_step": 1e3 * el / steps,
-            "sample": f"same workload at N={n} (dx={dx:.4g}), initialize + {warmup} untimed + {steps} timed steps,"
+            "sample": f"same workload at N={n}, initialize + {warmup} untimed + {steps} timed steps,"
                       f" {el:.2f} s; host {cpu_model}"}
 
 
@@ -384,10 +460,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--particles", type=float, default=1.0e6,
-                    help="workload size (profiling uses smaller cases of the same workload)")
+    ap.add_argument("--particles", type=float, default=0.0,
+                    help="workload size (default: the workload's own; profiling uses smaller cases)")
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--forms", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-clocks", action="store_true")
+    ap.add_argument("--verbose", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_setup(args.gpus)
@@ -396,12 +475,12 @@ def main():
         if rank != 0:
             return
         ref_steps = max(1, min(args.steps, 8))
-        cb = cpu_reference(ref_steps, 1)
+        cb = cpu_reference(ref_steps, 1, args.workload)
         line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": ref_steps,
                 "warmup": 1, "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak",
                 "device": "host cpu cores",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-                "config": {"workload": WORKLOAD, "sample": cb["sample"]},
+                "config": {"workload": WORKLOADS[args.workload].desc, "sample": cb["sample"]},
                 "cpu_baseline": cb,
                 "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -410,7 +489,8 @@ def main():
     out = run_gpu(args, rank, world, local)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
-            out["cpu_baseline"] = cpu_reference(2, 1)
+            log("cpu baseline")
+            out["cpu_baseline"] = cpu_reference(2, 1, args.workload)
         print(json.dumps(out), flush=True)
     try:
         import torch.distributed as dist

@@ -269,9 +269,34 @@ int sphgpu_timestep_noalloc(const double* acc_xyz, const double* sml, int64_t n,
 enum { SPHGPU_MLP_IN = 5, SPHGPU_MLP_HIDDEN = 64, SPHGPU_MLP_LAYERS = 3 };
 /* Number of FP32 parameters (weights + biases) of the MLP. */
 int64_t sphgpu_mlp_param_count(void);
-/* Load / read FP32 master parameters (length sphgpu_mlp_param_count()). */
+/* Load / read FP32 master parameters (length sphgpu_mlp_param_count()):
+   W0[64][5], b0[64], W1[64][64], b1[64], W2[64][64], b2[64], w3[64], b3. */
 int sphgpu_mlp_set_params(sphgpu_ctx* ctx, const float* params);
 int sphgpu_mlp_get_params(sphgpu_ctx* ctx, float* params);
+/* Deterministic Glorot-uniform initialisation from a seed. */
+int sphgpu_mlp_init(sphgpu_ctx* ctx, uint64_t seed);
+/* Riemann states are rows of 7 doubles: u_L, rho_L, p_L, u_R, rho_R, p_R,
+   gamma (left = neighbour j side, right = particle i side, as the GSPH force
+   poses them, src/gsph/g_fluid_force.cpp:140).  Network output
+   y = log(p_star / p_L) per state (host arrays). */
+int sphgpu_mlp_predict(sphgpu_ctx* ctx, const double* states, int64_t n, float* y);
+/* Adam training on labelled states (mean squared error in y) with the
+   project's tensor-core forward/backward kernels; loss_history[epochs].
+   epochs = 0: write the full-data gradient of the current parameters to
+   grad_out[param_count] and its loss to loss_history[0]. */
+int sphgpu_mlp_train(sphgpu_ctx* ctx, const double* states, const double* pstar, int64_t n, int epochs,
+                     int batch, float lr, uint64_t seed, float* loss_history, float* grad_out);
+/* Riemann problems in bulk on the device: mode 0 = the reference's iterative
+   solver (src/gsph/g_fluid_force.cpp:209-304), 1 = learned guess + Newton
+   (fallback to mode 0), 2 = converged to 1e-13 (training labels), 3 = plain
+   start converged to 1e-10.  Outputs may be NULL except pstar. */
+int sphgpu_riemann_batch(sphgpu_ctx* ctx, const double* states, int64_t n, int mode, double* pstar,
+                         double* vstar, int32_t* iters, int32_t* fallbacks);
+/* Harvest pair states from the plain solver's own runs: subsequent
+   FluidForce calls append sampled pairs (records of 8 doubles: the 7 state
+   values then p_star); harvest_end copies them out and stops. */
+int sphgpu_harvest_begin(sphgpu_ctx* ctx, int64_t capacity, uint32_t sample_mod);
+int sphgpu_harvest_end(sphgpu_ctx* ctx, double* out, int64_t capacity, int64_t* count);
 
 /* ---------------- workload generators (inputs, not the hot path) ------- */
 /* Deterministic initial conditions in the field order above; call with

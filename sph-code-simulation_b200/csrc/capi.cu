@@ -379,6 +379,11 @@ int sphgpu_destroy(sphgpu_ctx* c)
     if(c->stream) cudaStreamSynchronize(c->stream);
     free_all(c);
     if(c->d_mlp) cudaFree(c->d_mlp);
+    if(c->d_mlp_master) cudaFree(c->d_mlp_master);
+    if(c->d_mlp_feat) cudaFree(c->d_mlp_feat);
+    if(c->d_mlp_y) cudaFree(c->d_mlp_y);
+    if(c->d_harvest) cudaFree(c->d_harvest);
+    if(c->d_harvest_count) cudaFree(c->d_harvest_count);
     stage_flush(c);
     for(cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     for(cudaEvent_t e : c->user_ev) {

@@ -76,6 +76,7 @@ struct DevStatus {
     int max_count;         // largest list seen
     int node_pool;         // node pool exhausted
     int guard;             // a bounded device loop hit its limit (corrupt tree)
+    int nonfinite;         // a particle position is NaN or infinite
     unsigned long long newton_nonconv;
     unsigned long long riemann_solves;
     unsigned long long riemann_iters;

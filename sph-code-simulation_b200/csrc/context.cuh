@@ -57,9 +57,18 @@ struct sphgpu_ctx {
     sphgpu::DevStatus h_status{};
 
     // learned Riemann guess (BF16 weights + FP32 biases on device)
-    void* d_mlp = nullptr;
+    void* d_mlp = nullptr;            // BF16 / FP32 image read by the kernels
+    float* d_mlp_master = nullptr;    // FP32 master parameters + Adam moments
+    uint4* d_mlp_feat = nullptr;      // per pair slot: scaled features (bf16)
+    float* d_mlp_y = nullptr;         // per pair slot: network output
+    int64_t mlp_slots = 0;
     bool have_mlp = false;
     std::vector<float> mlp_master;
+    // pair-state harvesting (training data from the plain solver's own runs)
+    double* d_harvest = nullptr;
+    unsigned long long* d_harvest_count = nullptr;
+    int64_t harvest_cap = 0;
+    unsigned harvest_mod = 0;
 
     // counters kept on the host
     int64_t retries = 0;

@@ -114,17 +114,25 @@ __device__ void riemann_iterative(const double* L, const double* R, double gamma
     const double cr = sqrt(gamma * pr * rhor);
     double p;
     if(guess > 0.0) {
-        // learned start: Newton to 1e-10, FP32 iterations + FP64 check
-        p = guess;
-        bool ok = false;
-        for(int it = 0; it < budget; ++it) {
+        // Learned start.  Screen first with one Newton step from the
+        // reference's linearised guess: when that step moves p by less than
+        // 1 % the linearised start is already in Newton's quadratic range
+        // (nearly equal states, the common case inside a flow) and is kept;
+        // otherwise Newton restarts from the network's guess.  Either way
+        // Newton runs to a 1e-10 relative change within `budget` iterations,
+        // else the reference's solver takes over.
+        double q0 = pr - pl - cr * (ur - ul);
+        q0 = fmax(pl + q0 * cl / (cl + cr), 1e-25);
+        double q1 = vl_newton_step<double>(q0, ul, pl, vl, cl, ur, pr, vr, cr, g1, g2);
+        iters = 1;
+        const double ch = fabs(q1 - q0) / q1;
+        p = ch < 1e-2 ? q1 : guess;
+        bool ok = ch < 1e-10;
+        for(int it = 0; !ok && it < budget; ++it) {
             const double pold = p;
             p = vl_newton_step<double>(p, ul, pl, vl, cl, ur, pr, vr, cr, g1, g2);
             ++iters;
-            if(fabs(p - pold) / p < 1e-10) {
-                ok = true;
-                break;
-            }
+            if(fabs(p - pold) / p < 1e-10) ok = true;
         }
         if(ok) {
             pstar = p;
@@ -136,6 +144,7 @@ __device__ void riemann_iterative(const double* L, const double* R, double gamma
     double pg = pr - pl - cr * (ur - ul);
     pg = pl + pg * cl / (cl + cr);
     pg = fmax(pg, 1e-25);
+    // (after a failed learned start the counted iterations keep accumulating)
     if(sizeof(T) == sizeof(double)) {
         p = pg;
         for(int it = 0; it < 20; ++it) {
@@ -162,10 +171,12 @@ __device__ void riemann_iterative(const double* L, const double* R, double gamma
     vstar = vl_ustar(p, ul, pl, cl, ur, pr, cr, g1);
 }
 
-template <typename T, int G, int TYPE>
+// MODE: 0 = force (optionally harvesting pair states), 1 = GSPH features of
+// the learned guess only (no force written), 2 = force with the learned guess.
+template <typename T, int G, int TYPE, int MODE>
 __global__ void __launch_bounds__(FBLK) k_force(DevParams P, DevState S, int n, const int* __restrict__ list,
                                                 const int* __restrict__ count, int cap, const double* __restrict__ dtp,
-                                                DevStatus* __restrict__ st, MlpDev mlp)
+                                                DevStatus* __restrict__ st, MlpPairs mp, Harvest hv)
 {
     constexpr int GPW = 32 / G;
     const int lane = threadIdx.x & (G - 1);
@@ -268,15 +279,49 @@ __global__ void __launch_bounds__(FBLK) k_force(DevParams P, DevState S, int n, 
                     Lst[2] = tj.y;
                     Lst[3] = tj.w;
                 }
+                if(MODE == 1) {
+                    float x[MLP_IN];
+                    const bool ok = Lst[1] > 0.0 && Rst[1] > 0.0 && Lst[2] > 0.0 && Rst[2] > 0.0;
+                    if(ok) mlp_features(Lst, Rst, gamma, x);
+                    uint4 v;
+                    v.x = ok ? pack_bf16x2(x[0], x[1]) : 0u;
+                    v.y = ok ? pack_bf16x2(x[2], x[3]) : 0u;
+                    v.z = ok ? pack_bf16x2(x[4], 0.f) : 0u;
+                    v.w = 0u;
+                    mp.feat[(size_t)i * cap + k] = v;
+                    continue;
+                }
                 double pstar, vstar;
                 if(P.riemann == SPHGPU_RIEMANN_ITERATIVE) {
                     double guess = -1.0;
-                    if(mlp.w != nullptr) guess = mlp_guess(mlp, Lst, Rst, gamma);
+                    if(MODE == 2 && Lst[1] > 0.0 && Rst[1] > 0.0 && Lst[2] > 0.0 && Rst[2] > 0.0) {
+                        guess = Lst[2] * exp((double)mp.y[(size_t)i * cap + k]);
+                    }
                     int it = 0, fb = 0;
                     riemann_iterative<T>(Lst, Rst, gamma, guess, P.mlp_max_newton, pstar, vstar, it, fb);
                     ++solves;
                     iters += it;
                     fallbacks += fb;
+                    if(MODE == 0 && hv.mod) {
+                        unsigned hsh = (unsigned)i * 0x9E3779B1u ^ (unsigned)k * 0x85EBCA77u ^ hv.salt;
+                        hsh ^= hsh >> 15;
+                        hsh *= 0x2C1B3C6Du;
+                        hsh ^= hsh >> 12;
+                        if(hsh % hv.mod == 0) {
+                            const unsigned long long slot = atomicAdd(hv.count, 1ull);
+                            if((long long)slot < hv.cap) {
+                                double* o = hv.out + 8 * slot;
+                                o[0] = Lst[0];
+                                o[1] = Lst[1];
+                                o[2] = Lst[2];
+                                o[3] = Rst[0];
+                                o[4] = Rst[1];
+                                o[5] = Rst[2];
+                                o[6] = gamma;
+                                o[7] = pstar;
+                            }
+                        }
+                    }
                 } else if(sizeof(T) == sizeof(double)) {
                     riemann_hll<double>(Lst, Rst, pstar, vstar);
                 } else {
@@ -343,9 +388,9 @@ __global__ void __launch_bounds__(FBLK) k_force(DevParams P, DevState S, int n, 
         ay = group_sum<G>(ay);
         az = group_sum<G>(az);
         de = group_sum<G>(de);
-        if(valid && lane == 0) S.acc[i] = make_double4(ax, ay, az, de);
+        if(MODE != 1 && valid && lane == 0) S.acc[i] = make_double4(ax, ay, az, de);
     }
-    if(TYPE == SPHGPU_GSPH) {
+    if(TYPE == SPHGPU_GSPH && MODE != 1) {
         for(int o = 16; o > 0; o >>= 1) {
             solves += __shfl_xor_sync(FULL_MASK, solves, o);
             iters += __shfl_xor_sync(FULL_MASK, iters, o);
@@ -368,21 +413,63 @@ unsigned force_grid(int n)
     return (unsigned)std::max<long long>(1, std::min<long long>(blocks, 148LL * 8 * 4));
 }
 
-template <typename T>
-void launch_force(sphgpu_ctx* c, MlpDev m)
+template <typename T, int MODE>
+void launch_force(sphgpu_ctx* c, MlpPairs mp, Harvest hv)
 {
     const unsigned grid = force_grid(c->n);
     const int type = c->prm.sph_type;
     if(type == SPHGPU_DISPH) {
-        k_force<T, GROUP, SPHGPU_DISPH><<<grid, FBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_plist, c->d_pcount,
-                                                                      (int)c->pcap, c->d_dt, c->d_status, m);
+        k_force<T, GROUP, SPHGPU_DISPH, 0><<<grid, FBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_plist, c->d_pcount,
+                                                                         (int)c->pcap, c->d_dt, c->d_status, mp, hv);
     } else if(type == SPHGPU_GSPH) {
-        k_force<T, GROUP, SPHGPU_GSPH><<<grid, FBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_plist, c->d_pcount,
-                                                                     (int)c->pcap, c->d_dt, c->d_status, m);
+        k_force<T, GROUP, SPHGPU_GSPH, MODE><<<grid, FBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_plist,
+                                                                           c->d_pcount, (int)c->pcap, c->d_dt,
+                                                                           c->d_status, mp, hv);
     } else {
-        k_force<T, GROUP, SPHGPU_SSPH><<<grid, FBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_plist, c->d_pcount,
-                                                                     (int)c->pcap, c->d_dt, c->d_status, m);
+        k_force<T, GROUP, SPHGPU_SSPH, 0><<<grid, FBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_plist, c->d_pcount,
+                                                                        (int)c->pcap, c->d_dt, c->d_status, mp, hv);
     }
+}
+
+// Riemann problems in bulk (labels and evaluation of the learned guess).
+// states: n x 7 (u_L, rho_L, p_L, u_R, rho_R, p_R, gamma).
+__global__ void k_riemann_batch(const double* __restrict__ st, long long n, int mode, const float* __restrict__ y,
+                                int budget, double* __restrict__ pstar, double* __restrict__ vstar,
+                                int* __restrict__ iters, int* __restrict__ fb)
+{
+    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(r >= n) return;
+    const double* s = st + 7 * r;
+    const double gamma = s[6];
+    const double L[4] = {s[0], s[1], s[2], sqrt(gamma * s[2] / s[1])};
+    const double R[4] = {s[3], s[4], s[5], sqrt(gamma * s[5] / s[4])};
+    double p = 0.0, v = 0.0;
+    int it = 0, f = 0;
+    if(mode == 0) {
+        riemann_iterative<double>(L, R, gamma, -1.0, budget, p, v, it, f);
+    } else if(mode == 1) {
+        riemann_iterative<double>(L, R, gamma, L[2] * exp((double)y[r]), budget, p, v, it, f);
+    } else {
+        // plain start, Newton to a relative change of 1e-13 (mode 2, labels)
+        // or 1e-10 (mode 3, the learned path's target accuracy)
+        const double tol = mode == 2 ? 1e-13 : 1e-10;
+        const double g2 = 1.0 + gamma, g1 = 0.5 * g2 / gamma;
+        const double cl = sqrt(gamma * L[2] * L[1]), cr = sqrt(gamma * R[2] * R[1]);
+        double q = R[2] - L[2] - cr * (R[0] - L[0]);
+        q = fmax(L[2] + q * cl / (cl + cr), 1e-25);
+        for(int k = 0; k < 100; ++k) {
+            const double qo = q;
+            q = vl_newton_step<double>(q, L[0], L[2], 1.0 / L[1], cl, R[0], R[2], 1.0 / R[1], cr, g1, g2);
+            ++it;
+            if(fabs(q - qo) / q < tol) break;
+        }
+        p = q;
+        v = vl_ustar(q, L[0], L[2], cl, R[0], R[2], cr, g1);
+    }
+    pstar[r] = p;
+    if(vstar) vstar[r] = v;
+    if(iters) iters[r] = it;
+    if(fb) fb[r] = f;
 }
 
 }  // namespace
@@ -390,19 +477,122 @@ void launch_force(sphgpu_ctx* c, MlpDev m)
 int fluid_force(sphgpu_ctx* c)
 {
     if(!c->have_tree) return fail(c, SPHGPU_ERR_STATE, "FluidForce before tree make");
-    MlpDev m{};
-    if(c->prm.riemann_guess == SPHGPU_GUESS_MLP && c->prm.sph_type == SPHGPU_GSPH) {
-        if(!c->have_mlp) return fail(c, SPHGPU_ERR_NO_MLP, "learned Riemann guess requested without MLP weights");
-        m = mlp_device(c);
-    }
+    const bool learned = c->prm.riemann_guess == SPHGPU_GUESS_MLP && c->prm.sph_type == SPHGPU_GSPH &&
+                         c->prm.riemann_solver == SPHGPU_RIEMANN_ITERATIVE;
+    if(learned && !c->have_mlp) return fail(c, SPHGPU_ERR_NO_MLP, "learned Riemann guess requested without MLP weights");
     const int rc_walk = pair_walk(c);
     if(rc_walk < 0) return rc_walk;
     stage_begin(c, SPHGPU_T_FORCE);
-    if(c->prm.precision == SPHGPU_MIXED) launch_force<float>(c, m);
-    else launch_force<double>(c, m);
+    Harvest hv{c->d_harvest, c->d_harvest_count, c->harvest_cap, c->harvest_mod, 0u};
+    MlpPairs mp{nullptr, nullptr};
+    int launches = 1;
+    if(learned) {
+        const int64_t slots = (int64_t)c->n * c->pcap;
+        if(slots > c->mlp_slots) {
+            if(c->d_mlp_feat) cudaFree(c->d_mlp_feat);
+            if(c->d_mlp_y) cudaFree(c->d_mlp_y);
+            c->d_mlp_feat = nullptr;
+            c->d_mlp_y = nullptr;
+            SPHGPU_CUDA(c, cudaMalloc(&c->d_mlp_feat, sizeof(uint4) * (size_t)slots));
+            SPHGPU_CUDA(c, cudaMalloc(&c->d_mlp_y, sizeof(float) * (size_t)slots));
+            c->mlp_slots = slots;
+        }
+        mp.feat = c->d_mlp_feat;
+        mp.y = c->d_mlp_y;
+        if(c->prm.precision == SPHGPU_MIXED) launch_force<float, 1>(c, mp, hv);
+        else launch_force<double, 1>(c, mp, hv);
+        const int rc = mlp_infer_pairs(c, c->d_pcount, c->n, (int)c->pcap);
+        if(rc < 0) return rc;
+        if(c->prm.precision == SPHGPU_MIXED) launch_force<float, 2>(c, mp, hv);
+        else launch_force<double, 2>(c, mp, hv);
+        launches = 3;
+    } else {
+        if(c->prm.precision == SPHGPU_MIXED) launch_force<float, 0>(c, mp, hv);
+        else launch_force<double, 0>(c, mp, hv);
+    }
     SPHGPU_LAUNCH_CHECK(c, "FluidForce");
-    stage_end(c, SPHGPU_T_FORCE, 1);
+    stage_end(c, SPHGPU_T_FORCE, launches);
     return rc_walk;
 }
 
 }  // namespace sphgpu
+
+using namespace sphgpu;
+
+extern "C" {
+
+int sphgpu_riemann_batch(sphgpu_ctx* c, const double* states, int64_t n, int mode, double* pstar, double* vstar,
+                         int32_t* iters, int32_t* fallbacks)
+{
+    if(!c || !states || !pstar || n <= 0 || mode < 0 || mode > 3) return SPHGPU_ERR_ARG;
+    if(!c->stream) return fail(c, SPHGPU_ERR_CUDA, "context has no device");
+    if(mode == 1 && !c->have_mlp) return fail(c, SPHGPU_ERR_NO_MLP, "no MLP parameters loaded");
+    double *d_st = nullptr, *d_p = nullptr, *d_v = nullptr;
+    int *d_it = nullptr, *d_fb = nullptr;
+    float* d_y = nullptr;
+    SPHGPU_CUDA(c, cudaMalloc(&d_st, sizeof(double) * 7 * (size_t)n));
+    SPHGPU_CUDA(c, cudaMemcpyAsync(d_st, states, sizeof(double) * 7 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    SPHGPU_CUDA(c, cudaMalloc(&d_p, sizeof(double) * (size_t)n));
+    SPHGPU_CUDA(c, cudaMalloc(&d_v, sizeof(double) * (size_t)n));
+    SPHGPU_CUDA(c, cudaMalloc(&d_it, sizeof(int) * (size_t)n));
+    SPHGPU_CUDA(c, cudaMalloc(&d_fb, sizeof(int) * (size_t)n));
+    if(mode == 1) {
+        SPHGPU_CUDA(c, cudaMalloc(&d_y, sizeof(float) * (size_t)n));
+        const int rc = mlp_predict_states(c, d_st, n, d_y);
+        if(rc < 0) return rc;
+    }
+    const int budget = mode == 1 ? c->prm.mlp_max_newton : 20;
+    k_riemann_batch<<<grid_for(n, 256), 256, 0, c->stream>>>(d_st, n, mode, d_y, budget, d_p, d_v, d_it, d_fb);
+    SPHGPU_LAUNCH_CHECK(c, "riemann batch");
+    SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));  // the context stream does not sync with cudaMemcpy
+    SPHGPU_CUDA(c, cudaMemcpy(pstar, d_p, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost));
+    if(vstar) SPHGPU_CUDA(c, cudaMemcpy(vstar, d_v, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost));
+    if(iters) SPHGPU_CUDA(c, cudaMemcpy(iters, d_it, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost));
+    if(fallbacks) SPHGPU_CUDA(c, cudaMemcpy(fallbacks, d_fb, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost));
+    cudaFree(d_st);
+    cudaFree(d_p);
+    cudaFree(d_v);
+    cudaFree(d_it);
+    cudaFree(d_fb);
+    if(d_y) cudaFree(d_y);
+    return SPHGPU_OK;
+}
+
+// Collect pair states from the plain solver: the next FluidForce calls
+// append every pair with hash(i, k) % sample_mod == 0 (up to capacity
+// records of 8 doubles).  sphgpu_harvest_end copies them out and stops.
+int sphgpu_harvest_begin(sphgpu_ctx* c, int64_t capacity, uint32_t sample_mod)
+{
+    if(!c || capacity <= 0 || sample_mod == 0) return SPHGPU_ERR_ARG;
+    if(c->d_harvest) cudaFree(c->d_harvest);
+    if(c->d_harvest_count) cudaFree(c->d_harvest_count);
+    SPHGPU_CUDA(c, cudaMalloc(&c->d_harvest, sizeof(double) * 8 * (size_t)capacity));
+    SPHGPU_CUDA(c, cudaMalloc(&c->d_harvest_count, sizeof(unsigned long long)));
+    SPHGPU_CUDA(c, cudaMemsetAsync(c->d_harvest_count, 0, sizeof(unsigned long long), c->stream));
+    SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->harvest_cap = capacity;
+    c->harvest_mod = sample_mod;
+    return SPHGPU_OK;
+}
+
+int sphgpu_harvest_end(sphgpu_ctx* c, double* out, int64_t capacity, int64_t* count)
+{
+    if(!c || !count) return SPHGPU_ERR_ARG;
+    *count = 0;
+    if(!c->d_harvest) return fail(c, SPHGPU_ERR_STATE, "no harvest in progress");
+    unsigned long long n = 0;
+    SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    SPHGPU_CUDA(c, cudaMemcpy(&n, c->d_harvest_count, sizeof(n), cudaMemcpyDeviceToHost));
+    const int64_t m = std::min<int64_t>(std::min<int64_t>((int64_t)n, c->harvest_cap), capacity);
+    if(out && m > 0) SPHGPU_CUDA(c, cudaMemcpy(out, c->d_harvest, sizeof(double) * 8 * (size_t)m, cudaMemcpyDeviceToHost));
+    *count = m;
+    cudaFree(c->d_harvest);
+    cudaFree(c->d_harvest_count);
+    c->d_harvest = nullptr;
+    c->d_harvest_count = nullptr;
+    c->harvest_cap = 0;
+    c->harvest_mod = 0;
+    return SPHGPU_OK;
+}
+
+}  // extern "C"

@@ -41,13 +41,16 @@ namespace {
 constexpr int BLK = 256;
 
 // ---------------------------------------------------------------- bbox
-__global__ void k_bbox_partial(const double4* __restrict__ pos, int n, double* __restrict__ part)
+__global__ void k_bbox_partial(const double4* __restrict__ pos, int n, double* __restrict__ part,
+                               DevStatus* __restrict__ st)
 {
     __shared__ double smin[3][BLK], smax[3][BLK];
     double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
     for(int i = blockIdx.x * BLK + threadIdx.x; i < n; i += gridDim.x * BLK) {
         const double4 p = pos[i];
         const double v[3] = {p.x, p.y, p.z};
+        // a non-finite coordinate would collapse every key onto one path
+        if(!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) st->nonfinite = 1;
         for(int k = 0; k < 3; ++k) {
             if(mn[k] > v[k]) mn[k] = v[k];
             if(mx[k] < v[k]) mx[k] = v[k];
@@ -289,7 +292,11 @@ __global__ void k_nodes(const uint64_t* __restrict__ keys, int n, int D, const i
     leaf_of_start[p] = b + (leaf - lfirst);
 }
 
-// Reorder each leaf's particles into the reference's list order.
+// Reorder each leaf's particles into the reference's list order.  Small
+// leaves use insertion sort; large ones (coincident particles at the maximum
+// level) a heap sort, so the cost stays O(L log L) per leaf.
+__device__ __forceinline__ bool leaf_before(int a, int b, bool ascending) { return ascending ? a < b : a > b; }
+
 __global__ void k_leaf_order(int n, const int* __restrict__ leaf_of_start, const int4* __restrict__ link,
                              const int* __restrict__ old_id, uint32_t* __restrict__ vals)
 {
@@ -301,17 +308,39 @@ __global__ void k_leaf_order(int n, const int* __restrict__ leaf_of_start, const
     const int cnt = lk.y - lk.x;
     if(cnt <= 1) return;
     const bool ascending = ((lk.w & 0xff) & 1) != 0;
-    for(int a = lk.x + 1; a < lk.y; ++a) {
-        const uint32_t v = vals[a];
-        const int key = old_id[v];
-        int b = a - 1;
-        while(b >= lk.x) {
-            const int kb = old_id[vals[b]];
-            if(ascending ? (kb <= key) : (kb >= key)) break;
-            vals[b + 1] = vals[b];
-            --b;
+    uint32_t* v = vals + lk.x;
+    if(cnt <= 32) {
+        for(int a = 1; a < cnt; ++a) {
+            const uint32_t x = v[a];
+            const int key = old_id[x];
+            int b = a - 1;
+            while(b >= 0 && leaf_before(key, old_id[v[b]], ascending)) {
+                v[b + 1] = v[b];
+                --b;
+            }
+            v[b + 1] = x;
         }
-        vals[b + 1] = v;
+        return;
+    }
+    // heap sort (ids are unique, so stability is not needed)
+    auto sift = [&](int root, int end) {
+        while(true) {
+            int child = 2 * root + 1;
+            if(child >= end) break;
+            if(child + 1 < end && leaf_before(old_id[v[child]], old_id[v[child + 1]], ascending)) ++child;
+            if(!leaf_before(old_id[v[root]], old_id[v[child]], ascending)) break;
+            const uint32_t t = v[root];
+            v[root] = v[child];
+            v[child] = t;
+            root = child;
+        }
+    };
+    for(int r = cnt / 2 - 1; r >= 0; --r) sift(r, cnt);
+    for(int end = cnt - 1; end > 0; --end) {
+        const uint32_t t = v[0];
+        v[0] = v[end];
+        v[end] = t;
+        sift(0, end);
     }
 }
 
@@ -446,10 +475,9 @@ int tree_make(sphgpu_ctx* c)
     // root cube
     const int nb = (int)std::min<long long>(grid_for(n, BLK), 1024);
     int launches = 3;  // root, keys, levels
-    if(!c->prm.periodic) {
-        k_bbox_partial<<<nb, BLK, 0, st>>>(c->s.pos, n, c->d_bbox_part);
-        ++launches;
-    }
+    SPHGPU_CUDA(c, cudaMemsetAsync(&c->d_status->nonfinite, 0, sizeof(int), st));
+    k_bbox_partial<<<nb, BLK, 0, st>>>(c->s.pos, n, c->d_bbox_part, c->d_status);
+    ++launches;
     k_root<<<1, 32, 0, st>>>(c->d_bbox_part, nb, c->dp, c->d_root);
     // keys + sort
     k_keys<<<grid_for(n, BLK), BLK, 0, st>>>(c->s.pos, n, c->d_root, D, c->d_keys, c->d_vals);
@@ -466,6 +494,10 @@ int tree_make(sphgpu_ctx* c)
     int nnodes = 0;
     SPHGPU_CUDA(c, cudaMemcpyAsync(&nnodes, c->t.nnodes, sizeof(int), cudaMemcpyDeviceToHost, st));
     SPHGPU_CUDA(c, cudaStreamSynchronize(st));
+    if(c->h_status.nonfinite) {
+        c->have_tree = false;
+        return fail(c, SPHGPU_ERR_STATE, "non-finite particle position");
+    }
     if(c->h_status.node_pool) {
         c->have_tree = false;
         return fail(c, SPHGPU_ERR_NODE_POOL, "There is no free node.");

@@ -138,6 +138,13 @@ def lib() -> C.CDLL:
         "sphgpu_mlp_param_count": (i64, []),
         "sphgpu_mlp_set_params": (C.c_int, [vp, C.POINTER(C.c_float)]),
         "sphgpu_mlp_get_params": (C.c_int, [vp, C.POINTER(C.c_float)]),
+        "sphgpu_mlp_init": (C.c_int, [vp, C.c_uint64]),
+        "sphgpu_mlp_predict": (C.c_int, [vp, dp, i64, C.POINTER(C.c_float)]),
+        "sphgpu_mlp_train": (C.c_int, [vp, dp, dp, i64, C.c_int, C.c_int, C.c_float, C.c_uint64,
+                                       C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+        "sphgpu_riemann_batch": (C.c_int, [vp, dp, i64, C.c_int, dp, dp, i32p, i32p]),
+        "sphgpu_harvest_begin": (C.c_int, [vp, i64, C.c_uint32]),
+        "sphgpu_harvest_end": (C.c_int, [vp, dp, i64, i64p]),
         "sphgpu_sample_evrard": (i64, [C.c_int, C.c_double, C.c_double, dpp]),
         "sphgpu_sample_shear_layer": (i64, [C.c_double, C.c_double, C.c_double, dpp]),
         "sphgpu_sample_shock_tube": (i64, [C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, dpp]),
@@ -372,6 +379,57 @@ class Simulation:
         if p.size != lib().sphgpu_mlp_param_count():
             raise ValueError("wrong MLP parameter count")
         self._check(lib().sphgpu_mlp_set_params(self._h, p.ctypes.data_as(C.POINTER(C.c_float))), "mlp_set_params")
+
+    def load_riemann_mlp(self, path: Optional[str] = None):
+        """Load trained weights (default: riemann_mlp_weights.npy beside this file)."""
+        path = path or os.path.join(HERE, "riemann_mlp_weights.npy")
+        self.mlp_set_params(np.load(path))
+
+    def mlp_init(self, seed: int = 12345):
+        self._check(lib().sphgpu_mlp_init(self._h, seed), "mlp_init")
+
+    def mlp_predict(self, states: np.ndarray) -> np.ndarray:
+        st = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 7)
+        y = np.zeros(len(st), dtype=np.float32)
+        self._check(lib().sphgpu_mlp_predict(self._h, st.ctypes.data_as(C.POINTER(C.c_double)), len(st),
+                                             y.ctypes.data_as(C.POINTER(C.c_float))), "mlp_predict")
+        return y
+
+    def mlp_train(self, states: np.ndarray, pstar: np.ndarray, epochs: int, batch: int = 16384,
+                  lr: float = 2e-3, seed: int = 12345):
+        """Train; epochs = 0 returns (loss, gradient) of the current parameters."""
+        st = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 7)
+        ps = np.ascontiguousarray(pstar, dtype=np.float64)
+        hist = np.zeros(max(epochs, 1), dtype=np.float32)
+        grad = np.zeros(lib().sphgpu_mlp_param_count(), dtype=np.float32)
+        fp = C.POINTER(C.c_float)
+        self._check(lib().sphgpu_mlp_train(self._h, st.ctypes.data_as(C.POINTER(C.c_double)),
+                                           ps.ctypes.data_as(C.POINTER(C.c_double)), len(st), epochs, batch, lr,
+                                           seed, hist.ctypes.data_as(fp), grad.ctypes.data_as(fp)), "mlp_train")
+        return (hist[0], grad) if epochs == 0 else hist
+
+    def riemann_batch(self, states: np.ndarray, mode: int):
+        """(p*, v*, iterations, fallbacks) for n x 7 states; mode as in sphgpu.h."""
+        st = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 7)
+        n = len(st)
+        p, v = np.zeros(n), np.zeros(n)
+        it, fb = np.zeros(n, dtype=np.int32), np.zeros(n, dtype=np.int32)
+        dp_ = C.POINTER(C.c_double)
+        i32p = C.POINTER(C.c_int32)
+        self._check(lib().sphgpu_riemann_batch(self._h, st.ctypes.data_as(dp_), n, mode, p.ctypes.data_as(dp_),
+                                               v.ctypes.data_as(dp_), it.ctypes.data_as(i32p),
+                                               fb.ctypes.data_as(i32p)), "riemann_batch")
+        return p, v, it, fb
+
+    def harvest_begin(self, capacity: int, sample_mod: int):
+        self._check(lib().sphgpu_harvest_begin(self._h, capacity, sample_mod), "harvest_begin")
+
+    def harvest_end(self, capacity: int) -> np.ndarray:
+        out = np.zeros((capacity, 8))
+        cnt = C.c_int64()
+        self._check(lib().sphgpu_harvest_end(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), capacity,
+                                             C.byref(cnt)), "harvest_end")
+        return out[: cnt.value]
 
     def mlp_get_params(self) -> np.ndarray:
         p = np.zeros(lib().sphgpu_mlp_param_count(), dtype=np.float32)

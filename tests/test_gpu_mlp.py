@@ -1,0 +1,123 @@
+"""The learned Riemann guess: tensor-core forward / backward against the CPU
+FP64 oracle (oracle/mlp_oracle.py), training, and the gain over the plain
+iterative solver."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def M():
+    import mlp_oracle
+    return mlp_oracle
+
+
+def _sim(gpu, **kw):
+    p = gpu.config_params("tube_gsph", **kw)
+    return gpu.Simulation(p)
+
+
+def test_forward_matches_oracle(gpu, M):
+    states = M.random_states(4096, seed=7)
+    with _sim(gpu) as sim:
+        sim.mlp_init(3)
+        params = sim.mlp_get_params()
+        y = sim.mlp_predict(states)
+    x = M.features(states)
+    y_bf16, _ = M.forward(params, x, emulate_bf16=True)
+    y_f64, _ = M.forward(params, x, emulate_bf16=False)
+    # bf16 weights / activations are the model; against the emulation only
+    # FP32 accumulation order and the exp of SiLU differ
+    assert np.max(np.abs(y - y_bf16)) < 2e-2
+    assert np.median(np.abs(y - y_bf16)) < 2e-3
+    assert np.max(np.abs(y - y_f64)) < 1e-1
+
+
+def test_gradient_matches_oracle(gpu, M):
+    states = M.random_states(2048, seed=11)
+    with _sim(gpu) as sim:
+        p_lab, _, _, _ = sim.riemann_batch(states, mode=2)
+        sim.mlp_init(5)
+        params = sim.mlp_get_params()
+        loss, grad = sim.mlp_train(states, p_lab, epochs=0)
+    x = M.features(states)
+    t = np.log(p_lab / states[:, 2]).astype(np.float32).astype(np.float64)
+    l_ref, g_ref = M.loss_and_grad(params, x, t, emulate_bf16=True)
+    assert loss == pytest.approx(l_ref, rel=2e-2)
+    blocks = [(0, 320), (320, 384), (384, 4480), (4480, 4544), (4544, 8640), (8640, 8704), (8704, 8768),
+              (8768, 8769)]
+    for a, b in blocks:
+        gg, gr = grad[a:b].astype(np.float64), g_ref[a:b]
+        rel = np.linalg.norm(gg - gr) / max(np.linalg.norm(gr), 1e-30)
+        cos = gg @ gr / max(np.linalg.norm(gg) * np.linalg.norm(gr), 1e-30)
+        assert rel < 3e-2 and cos > 0.999, (a, b, rel, cos)
+
+
+def test_training_reduces_loss(gpu, M):
+    train = M.random_states(300_000, seed=12345)
+    with _sim(gpu) as sim:
+        p_tr, _, it_tr, _ = sim.riemann_batch(train, mode=2)
+        keep = (p_tr > 1e-20) & (it_tr < 100)
+        sim.mlp_init(12345)
+        hist = sim.mlp_train(train[keep], p_tr[keep], epochs=12, batch=8192, lr=2e-3)
+    assert np.all(np.isfinite(hist))
+    assert hist[-1] < 0.2 * hist[0]
+
+
+def test_shipped_network_gains_over_plain_solver(gpu, M):
+    """The trained network (riemann_mlp_weights.npy, made by
+    train_riemann_mlp.py) on held-out random states: fewer Newton iterations
+    than the plain start to the same 1e-10 accuracy, rare fallbacks."""
+    test = M.random_states(100_000, seed=999)
+    with _sim(gpu) as sim:
+        sim.load_riemann_mlp()
+        p_ref, _, it_ref, _ = sim.riemann_batch(test, mode=2)
+        ok = (p_ref > 1e-20) & (it_ref < 100)
+        test, p_ref = test[ok], p_ref[ok]
+        p_plain, _, it_plain, _ = sim.riemann_batch(test, mode=3)   # plain start, same 1e-10 target
+        p_ml, _, it_ml, fb = sim.riemann_batch(test, mode=1)
+    rel = np.abs(p_ml - p_ref) / p_ref
+    assert np.median(rel) < 1e-12 and np.quantile(rel, 0.999) < 1e-8
+    assert fb.mean() < 0.01
+    assert it_ml.mean() < 0.85 * it_plain.mean()
+
+
+def test_gsph_force_with_learned_guess(gpu):
+    p = gpu.config_params("tube_gsph", range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.1, 0.1))
+    fields = gpu.sample_shock_tube(0.02, ly=0.1)
+    out = {}
+    for guess in (gpu.GUESS_NONE, gpu.GUESS_MLP):
+        p.riemann_guess = guess
+        with gpu.Simulation(p) as sim:
+            if guess == gpu.GUESS_MLP:
+                import mlp_oracle as M
+                st = M.random_states(100_000, seed=1)
+                pl, _, it, _ = sim.riemann_batch(st, mode=2)
+                keep = pl > 1e-20
+                sim.mlp_init(1)
+                sim.mlp_train(st[keep], pl[keep], epochs=4, batch=8192)
+            sim.upload(fields)
+            sim.initialize()
+            sim.integrate()
+            out[guess] = (sim.download(), sim.counters())
+    a0, c0 = out[gpu.GUESS_NONE]
+    a1, c1 = out[gpu.GUESS_MLP]
+    amax = max(np.max(np.abs(a0["acc_" + k])) for k in "xyz")
+    for k in "xyz":
+        assert np.max(np.abs(a1["acc_" + k] - a0["acc_" + k])) / amax < 1e-4
+    assert c1["riemann_solves"] == c0["riemann_solves"]
+
+
+def test_harvest_pair_states(gpu):
+    p = gpu.config_params("tube_gsph", range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.1, 0.1))
+    fields = gpu.sample_shock_tube(0.02, ly=0.1)
+    with gpu.Simulation(p) as sim:
+        sim.upload(fields)
+        sim.initialize()
+        sim.harvest_begin(100_000, 7)
+        sim.integrate()
+        rec = sim.harvest_end(100_000)
+        assert len(rec) > 100
+        p_again, _, _, _ = sim.riemann_batch(rec[:, :7], mode=0)
+    np.testing.assert_allclose(p_again, rec[:, 7], rtol=1e-12)
