@@ -240,7 +240,7 @@ def run_gpu(args, rank: int, world: int, local: int):
                 c = sim.counters()
                 log(f"warm-up step {w} done: max_gather {c['max_gather']} max_pair {c['max_pair']} "
                     f"cap {c['gather_capacity']} retries {c['retries']} nodes {c['node_count']} "
-                    f"lane_warps {c['walk_lane_warps']} fallbacks {c['walk_fallbacks']} dt {sim.time_dt()[1]:.3e}")
+                    f"split_warps {c['walk_split_warps']} fallbacks {c['walk_fallbacks']} dt {sim.time_dt()[1]:.3e}")
         sim.synchronize()
         sim.reset_counters()
         sim.enable_timing(True)
@@ -258,7 +258,7 @@ def run_gpu(args, rank: int, world: int, local: int):
                 c = sim.counters()
                 log(f"timed step {k}: max_gather {c['max_gather']} max_pair {c['max_pair']} "
                     f"cap {c['gather_capacity']} retries {c['retries']} nodes {c['node_count']} "
-                    f"lane_warps {c['walk_lane_warps']} fallbacks {c['walk_fallbacks']} dt {sim.time_dt()[1]:.3e}")
+                    f"split_warps {c['walk_split_warps']} fallbacks {c['walk_fallbacks']} dt {sim.time_dt()[1]:.3e}")
         import ctypes
         ms = ctypes.c_double()
         G.lib().sphgpu_timer_stop(sim._h, ctypes.byref(ms))

@@ -128,8 +128,8 @@ typedef struct sphgpu_counters {
     int64_t max_pair;              /* largest symmetric list                 */
     int64_t node_count;            /* octree nodes of the last tree_make     */
     int64_t retries;               /* neighbour walks re-run after growing   */
-    int64_t walk_group_warps;      /* warps that took the group walk         */
-    int64_t walk_lane_warps;       /* warps that took the per-lane walk      */
+    int64_t walk_group_warps;      /* warps walked as one group of 32        */
+    int64_t walk_split_warps;      /* warps walked as several sub-groups     */
     int64_t walk_fallbacks;        /* group walks redone per lane (overflow) */
 } sphgpu_counters;
 

@@ -168,7 +168,8 @@ int alloc_all(sphgpu_ctx* c, int n)
     if((rc = dalloc(c, c->t.geo, nc)) || (rc = dalloc(c, c->t.mass, nc)) || (rc = dalloc(c, c->t.ksize, nc))
        || (rc = dalloc(c, c->t.link, nc)) || (rc = dalloc(c, c->t.parent, nc)) || (rc = dalloc(c, c->t.nchild, nc))
        || (rc = dalloc(c, c->t.child, 8 * (size_t)nc))
-       || (rc = dalloc(c, c->t.counter, nc)) || (rc = dalloc(c, c->t.nnodes, 4)))
+       || (rc = dalloc(c, c->t.counter, nc)) || (rc = dalloc(c, c->t.nnodes, 4))
+       || (rc = dalloc(c, c->t.leaf_of, n)) || (rc = dalloc(c, c->t.pks, n)))
         return rc;
     if((rc = dalloc(c, c->d_root, 1)) || (rc = dalloc(c, c->d_bbox_part, 6 * 1024)) || (rc = dalloc(c, c->d_keys, n))
        || (rc = dalloc(c, c->d_keys_alt, n)) || (rc = dalloc(c, c->d_vals, n)) || (rc = dalloc(c, c->d_vals_alt, n))
@@ -680,7 +681,7 @@ int sphgpu_get_counters(sphgpu_ctx* c, sphgpu_counters* o)
     o->node_count = c->node_count;
     o->retries = c->retries;
     o->walk_group_warps = (int64_t)c->h_status.walk_group_warps;
-    o->walk_lane_warps = (int64_t)c->h_status.walk_lane_warps;
+    o->walk_split_warps = (int64_t)c->h_status.walk_split_warps;
     o->walk_fallbacks = c->walk_fallbacks;
     return SPHGPU_OK;
 }

@@ -67,6 +67,8 @@ struct DevTree {
     int* nchild;
     int* counter;
     int* nnodes;     // device scalar: total node count (root included)
+    int* leaf_of;    // per particle (tree order): the leaf holding it
+    double* pks;     // per particle: kernel_size of its leaf (set_kernel)
 };
 
 // Packed status words read back by the host after a module.
@@ -82,7 +84,7 @@ struct DevStatus {
     unsigned long long riemann_iters;
     unsigned long long riemann_fallbacks;
     unsigned long long walk_group_warps;   // warps that took the group walk
-    unsigned long long walk_lane_warps;    // warps that took the per-lane walk
+    unsigned long long walk_split_warps;   // warps walked as several sub-groups
 };
 
 // Read-only 32-byte load through the non-coherent path (two 16-byte halves).

@@ -378,6 +378,7 @@ __global__ void k_mass_up(int n, const int* __restrict__ leaf_of_start, DevTree 
         double m = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
         // assign() accumulated in the parent's list order = reverse of ours
         for(int q = lk.y - 1; q >= lk.x; --q) {
+            T.leaf_of[q] = node;
             const double4 pq = pos[q];
             m = __dadd_rn(m, pq.w);
             cx = __dadd_rn(cx, __dmul_rn(pq.x, pq.w));
@@ -440,6 +441,7 @@ __global__ void k_ksize_up(int n, const int* __restrict__ leaf_of_start, DevTree
             if(h > k) k = h;
         }
         T.ksize[node] = k;
+        for(int q = lk.x; q < lk.y; ++q) T.pks[q] = k;
     }
     for(int up = 0; node != 0; ++up) {
         if(up > 64) {

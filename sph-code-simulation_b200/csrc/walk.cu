@@ -5,16 +5,29 @@
 // leaf the radius test r^2 < h^2 on every particle of the leaf list, with
 // h = sml (gather) or max(sml, node.kernel_size) (is_ij).
 //
-// Warp-cooperative walk: a warp owns 32 consecutive particles in octree order
-// (spatially coherent) and scans the preorder node array once.  Each lane
-// keeps one bit per tree level: bit L says "my box test passed at the current
-// level-L ancestor".  A node at level L is live for a lane iff bits 1..L-1 are
-// all set — exactly the set of nodes the reference's recursion would visit
-// for that particle.  The warp descends into a node (index + 1) when any live
-// lane passes, else jumps over the subtree (skip pointer).  Every test is
-// evaluated in unfused FP64 (this file builds with -fmad=false) so each
-// lane's list equals the reference's list as a set, and even in order before
-// the reference's distance sort.
+// Two walks produce the same sets.
+//
+// Group walk (default, k_walk_group): a warp owns 32 consecutive particles in
+// octree order.  The warp traverses the tree once for the bounding box of its
+// particles (a conservative superset test, 32 nodes per step from a shared
+// memory stack), queues passing leaves, and queues whole nodes that are small
+// or lie inside the search box instead of descending into them.  Queued
+// particles are staged 32 at a time; every lane classifies them against its
+// own particle in FP32 with rigorously rounded thresholds (certainly inside /
+// certainly outside / a thin band at the radius), and only band pairs run the
+// reference's FP64 test, with the box tests replayed up the parent chain for
+// pairs on the radius.  Warps whose particles straddle a large octant
+// boundary are split into compact sub-groups walked one after another.
+//
+// Per-lane walk (k_walk, the fallback and cross-check): each lane keeps one
+// bit per tree level: bit L says "my box test passed at the current level-L
+// ancestor".  A node at level L is live for a lane iff bits 1..L-1 are all
+// set: exactly the set of nodes the reference's recursion would visit for
+// that particle.  The warp descends into a node (index + 1) when any live lane
+// passes, else jumps over the subtree (skip pointer).  Every test is evaluated
+// in unfused FP64 (this file builds with -fmad=false), so each lane's list
+// equals the reference's list as a set, and even in order before the
+// reference's distance sort.
 //
 // Lists go to an ELL buffer (capacity slots per particle, row-major).  A list
 // longer than the capacity is counted but not stored; the host grows the
@@ -135,15 +148,19 @@ __global__ void __launch_bounds__(WBLK) k_walk(DevParams P, DevState S, DevTree 
 // Only pairs with h_leaf - delta <= r_ij < h_leaf need the reference's tests,
 // which are then replayed exactly up the parent chain.
 //
-// Traversal is therefore done once per warp for the group's bounding box:
+// Traversal is therefore done once per (sub-)group for its bounding box:
 // each step the 32 lanes test 32 stack nodes in parallel (a conservative
 // superset test), push the children of passing internal nodes (LIFO stack in
-// shared memory) and queue passing leaves; queued leaves are tested in
-// batches, each lane against its own particle.  A stack overflow marks the
-// warp and the host re-runs the call with the per-lane walk.
+// shared memory) and queue passing leaves and whole nodes; queued particles
+// are classified in chunks of 32, each lane against its own particle.  Any
+// superset of the reference's candidates gives the same lists, because the
+// per-pair classification alone decides membership.  A stack overflow marks
+// the warp and the host re-runs the call with the per-lane walk.
 constexpr int GW_WARPS = 4;
 constexpr int GW_STACK = 1024;
 constexpr int GW_QUEUE = 64;
+constexpr int GW_WHOLE = 8;   // nodes with at most this many particles are queued whole
+constexpr double GW_SPLIT = 6.0;  // sub-group extent limit, in units of its largest radius
 
 __device__ __forceinline__ double interval_gap(double c, double lo, double hi)
 {
@@ -177,9 +194,13 @@ __global__ void __launch_bounds__(GW_WARPS * 32) k_walk_group(DevParams P, DevSt
 {
     __shared__ int s_stack[GW_WARPS][GW_STACK];
     __shared__ int s_queue[GW_WARPS][GW_QUEUE];
+    __shared__ float4 s_cf[GW_WARPS][32];
     __shared__ double4 s_cpos[GW_WARPS][32];
-    __shared__ int4 s_clink[GW_WARPS][32];
-    __shared__ double s_cks[GW_WARPS][32];
+    __shared__ int s_cid[GW_WARPS][32];
+    __shared__ float s_ctin[GW_WARPS][32];
+    __shared__ int s_loff[GW_WARPS][32];
+    __shared__ int s_lstart[GW_WARPS][32];
+    __shared__ double s_box[GW_WARPS][32][7];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int i = (blockIdx.x * GW_WARPS + w) * 32 + lane;
     const bool valid = i < n;
@@ -198,34 +219,47 @@ __global__ void __launch_bounds__(GW_WARPS * 32) k_walk_group(DevParams P, DevSt
             hi = S.vel[i].w;
         }
     }
-    // group bounding box and largest radius
-    double lo[3] = {valid ? xi : 1e300, valid ? yi : 1e300, valid ? zi : 1e300};
-    double up[3] = {valid ? xi : -1e300, valid ? yi : -1e300, valid ? zi : -1e300};
-    double hmax = valid ? hi : 0.0;
-    for(int o = 16; o > 0; o >>= 1) {
-        for(int k = 0; k < 3; ++k) {
-            lo[k] = fmin(lo[k], __shfl_xor_sync(FULL_MASK, lo[k], o));
-            up[k] = fmax(up[k], __shfl_xor_sync(FULL_MASK, up[k], o));
+    // Sub-groups.  A window of 32 octree-ordered particles that straddles a
+    // large octant boundary has a bounding box far wider than its particles'
+    // search spheres.  The warp is split into aligned sub-groups of s lanes
+    // (s = 32, 16, ..., 1: the largest s for which every sub-group's extent
+    // is at most GW_SPLIT times its largest radius) and the cooperative walk
+    // runs once per sub-group, all lanes traversing and staging, only the
+    // sub-group's lanes testing candidates.
+    const double own_lo[3] = {valid ? xi : 1e300, valid ? yi : 1e300, valid ? zi : 1e300};
+    const double own_up[3] = {valid ? xi : -1e300, valid ? yi : -1e300, valid ? zi : -1e300};
+    const double own_h = valid ? hi : 0.0;
+    int s = 1;
+    {
+        double l[3] = {own_lo[0], own_lo[1], own_lo[2]}, u[3] = {own_up[0], own_up[1], own_up[2]}, hm = own_h;
+        for(int o = 1; o < 32; o <<= 1) {
+            for(int k = 0; k < 3; ++k) {
+                l[k] = fmin(l[k], __shfl_xor_sync(FULL_MASK, l[k], o));
+                u[k] = fmax(u[k], __shfl_xor_sync(FULL_MASK, u[k], o));
+            }
+            hm = fmax(hm, __shfl_xor_sync(FULL_MASK, hm, o));
+            const double e = fmax(u[0] - l[0], fmax(u[1] - l[1], u[2] - l[2]));
+            if(__all_sync(FULL_MASK, e <= GW_SPLIT * hm)) s = 2 * o;
         }
-        hmax = fmax(hmax, __shfl_xor_sync(FULL_MASK, hmax, o));
     }
-    // A window of 32 octree-ordered particles that straddles a large octant
-    // boundary has a bounding box far wider than its particles' search
-    // spheres; such warps walk per lane instead.
-    const double extent = fmax(up[0] - lo[0], fmax(up[1] - lo[1], up[2] - lo[2]));
-    if(!(extent <= 4.0 * hmax)) {
-        const size_t row0 = (size_t)(valid ? i : 0) * (size_t)cap;
-        const int c0 = walk_lanes<IJ>(P, S, T, valid, xi, yi, zi, hi, list, row0, cap, st);
-        if(lane == 0) atomicAdd(&st->walk_lane_warps, 1ull);
-        if(valid) {
-            count[i] = c0;
-            if(c0 > cap) st->overflow = 1;
-            if(c0 > P.nngb * 1000) st->fatal = 1;
-            atomicMax(&st->max_count, c0);
+    {
+        // each sub-group's box and radius, kept in shared memory
+        double lo[3] = {own_lo[0], own_lo[1], own_lo[2]}, up[3] = {own_up[0], own_up[1], own_up[2]};
+        double hmax = own_h;
+        for(int o = 1; o < s; o <<= 1) {
+            for(int k = 0; k < 3; ++k) {
+                lo[k] = fmin(lo[k], __shfl_xor_sync(FULL_MASK, lo[k], o));
+                up[k] = fmax(up[k], __shfl_xor_sync(FULL_MASK, up[k], o));
+            }
+            hmax = fmax(hmax, __shfl_xor_sync(FULL_MASK, hmax, o));
         }
-        return;
+        if(lane % s == 0) {
+            double* b = s_box[w][lane / s];
+            b[0] = lo[0], b[1] = lo[1], b[2] = lo[2], b[3] = up[0], b[4] = up[1], b[5] = up[2], b[6] = hmax;
+        }
+        __syncwarp();
     }
-    if(lane == 0) atomicAdd(&st->walk_group_warps, 1ull);
+    if(lane == 0) atomicAdd(s == 32 ? &st->walk_group_warps : &st->walk_split_warps, 1ull);
     // safety margin for the fast acceptance (see above)
     const double4 root = ldg4(&T.geo[0]);
     const double scale = fmax(fabs(root.x), fmax(fabs(root.y), fabs(root.z))) + root.w;
@@ -233,129 +267,242 @@ __global__ void __launch_bounds__(GW_WARPS * 32) k_walk_group(DevParams P, DevSt
 
     const size_t row = (size_t)(valid ? i : 0) * (size_t)cap;
     int cnt = 0;
-    int sp = 0, nq = 0;
     bool overflow = false;
-    if(lane == 0) s_stack[w][0] = 0;
-    sp = 1;
-    __syncwarp();
-
-    auto process = [&](int nproc) {
-        // lanes load one queued leaf each, then every lane tests all of them
-        const int L = lane < nproc ? s_queue[w][lane] : -1;
-        if(L >= 0) {
-            const int4 lk = __ldg(&T.link[L]);
-            s_clink[w][lane] = make_int4(lk.x, lk.y, L, 0);
-            s_cpos[w][lane] = ldg4(&S.pos[lk.x]);
-            s_cks[w][lane] = IJ ? __ldg(&T.ksize[L]) : 0.0;
-        }
+    for(int sg = 0; sg < 32 / s && !overflow; ++sg) {
+        const bool act = valid && lane / s == sg;
+        if(__ballot_sync(FULL_MASK, act) == 0) continue;
+        const double* bb = s_box[w][sg];
+        const double blo[3] = {bb[0], bb[1], bb[2]}, bup[3] = {bb[3], bb[4], bb[5]};
+        const double bh = bb[6];
+        const double bext = fmax(bup[0] - blo[0], fmax(bup[1] - blo[1], bup[2] - blo[2]));
+        int sp = 0, nq = 0;
+        if(lane == 0) s_stack[w][0] = 0;
+        sp = 1;
         __syncwarp();
-        if(valid) {
-            for(int t = 0; t < nproc; ++t) {
-                const int4 cl = s_clink[w][t];
-                double h = hi;
-                if(IJ) {
-                    const double ks = s_cks[w][t];
-                    h = hi < ks ? ks : hi;
-                }
-                const double h2 = h * h;
-                const double hs = h - delta;
-                const double hs2 = hs > 0.0 ? hs * hs : -1.0;
-                for(int q = cl.x; q < cl.y; ++q) {
-                    const double4 pj = q == cl.x ? s_cpos[w][t] : ldg4(&S.pos[q]);
-                    const Vec3d r = rij(P, xi, yi, zi, pj.x, pj.y, pj.z);
-                    const double r2 = abs2x(r);
-                    if(!(r2 < h2)) continue;
-                    bool take = r2 < hs2;
-                    if(!take) {
-                        // on the radius: replay the reference's box tests up the path
-                        take = true;
-                        int A = cl.z;
-                        for(int up_ = 0; A >= 0 && up_ < 64; ++up_) {
-                            if(!box_pass<IJ>(P, T, A, xi, yi, zi, hi)) {
-                                take = false;
-                                break;
-                            }
-                            A = A == 0 ? -1 : T.parent[A];
-                        }
+
+        // FP32 classification.  Candidates are staged once per warp as FP32
+        // offsets b_j = x_j - c from the group centre c (minimum image applied
+        // once, in FP64); each lane holds a_i = x_i - c.  For any candidate that
+        // can matter (|a_i - b_j| <~ h) the FP32 distance |a_i - b_j| differs from
+        // the exact r by at most E = 2^-22 ext + 2^-21 h (conversions and the
+        // subtraction; ext = sub-group extent) and the FP32 sum of squares r2f from
+        // |a_i - b_j|^2 by a factor 1 +- 3 * 2^-24.  Hence
+        //   r2f >= Tout(h) = ((1 + 2^-20) h + 2^-21 ext)^2 (1 + 2^-20)  =>  r >= h,
+        //   r2f <  Tin(h)  = ((1 - 2^-20) (h - delta - E))^2 (1 - 2^-20) =>  r < h - delta,
+        // both thresholds rounded outwards to FP32.  A pair below Tin is in the
+        // reference's set with every box test on its path passing (see above),
+        // so it is taken without FP64 work; only pairs between the thresholds run
+        // the exact FP64 test.  With periodic wrapping the FP32 offset is the
+        // minimum image only if |b_j| + ext/2 < L/2 on every axis (|a_i| <= ext/2);
+        // other candidates are staged with NaN offsets and always run the exact
+        // test.  Each lane classifies a chunk of 32 staged candidates branch-free
+        // into two bit masks (inside, band), runs the exact test for the band
+        // bits and writes the taken candidates in chunk order.
+        const double cx = 0.5 * (blo[0] + bup[0]), cy = 0.5 * (blo[1] + bup[1]), cz = 0.5 * (blo[2] + bup[2]);
+        const double ext_x = bup[0] - blo[0], ext_y = bup[1] - blo[1], ext_z = bup[2] - blo[2];
+        const float ax = (float)(xi - cx), ay = (float)(yi - cy), az = (float)(zi - cz);
+        auto t_out = [&](double h) -> float {
+            const double t = h * (1.0 + 0x1p-20) + 0x1p-21 * bext;
+            return __double2float_ru(t * t * (1.0 + 0x1p-20));
+        };
+        auto t_in = [&](double h) -> float {
+            const double t = (h - delta - (0x1p-22 * bext + 0x1p-21 * h)) * (1.0 - 0x1p-20);
+            return t > 0.0 ? __double2float_rd(t * t * (1.0 - 0x1p-20)) : -1.0f;
+        };
+        const float Ti_out = act ? t_out(hi) : -1.0f;
+        const float Ti_in = act ? t_in(hi) : -1.0f;
+        const float F_INF = __int_as_float(0x7f800000);
+        const float F_NAN = __int_as_float(0x7fffffff);
+
+        auto process = [&](int nproc) {
+            // expand the queued nodes into their particles (warp prefix sum)
+            int lstart = 0, lcnt = 0;
+            if(lane < nproc) {
+                const int4 lk = __ldg(&T.link[s_queue[w][lane]]);
+                lstart = lk.x;
+                lcnt = lk.y - lk.x;
+            }
+            int incl = lcnt;
+            for(int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(FULL_MASK, incl, o);
+                if(lane >= o) incl += u;
+            }
+            const int total = __shfl_sync(FULL_MASK, incl, 31);
+            s_loff[w][lane] = incl - lcnt;
+            s_lstart[w][lane] = lstart;
+            __syncwarp();
+            for(int base = 0; base < total; base += 32) {
+                const int g = base + lane;
+                if(g < total) {
+                    // the leaf holding candidate g: largest t < nproc with loff[t] <= g
+                    int t = 0;
+                    for(int s = 16; s > 0; s >>= 1) {
+                        if(t + s < nproc && s_loff[w][t + s] <= g) t += s;
                     }
-                    if(take) {
-                        if(cnt < cap) list[row + cnt] = q;
+                    const int q = s_lstart[w][t] + (g - s_loff[w][t]);
+                    const double4 pj = ldg4(&S.pos[q]);
+                    const double ks = IJ ? __ldg(&T.pks[q]) : 0.0;
+                    double bx = xsub(pj.x, cx), by = xsub(pj.y, cy), bz = xsub(pj.z, cz);
+                    bool pre = true;
+                    if(P.periodic) {
+                        bx = min_image(bx, P.range[0]);
+                        by = min_image(by, P.range[1]);
+                        bz = min_image(bz, P.range[2]);
+                        pre = fabs(bx) + 0.5 * ext_x < 0.499999 * P.range[0]
+                            && fabs(by) + 0.5 * ext_y < 0.499999 * P.range[1]
+                            && fabs(bz) + 0.5 * ext_z < 0.499999 * P.range[2];
+                    }
+                    float tko = -1.0f, tki = -1.0f;
+                    if(IJ) {
+                        tko = t_out(ks);
+                        tki = t_in(ks);
+                    }
+                    float fx = (float)bx, fy = (float)by, fz = (float)bz;
+                    if(!pre) fx = fy = fz = F_NAN;  // classified as band: exact test
+                    s_cf[w][lane] = make_float4(fx, fy, fz, tko);
+                    s_ctin[w][lane] = tki;
+                    s_cpos[w][lane] = make_double4(pj.x, pj.y, pj.z, ks);
+                    s_cid[w][lane] = q;
+                } else {
+                    // padding: infinitely far, never taken
+                    s_cf[w][lane] = make_float4(F_INF, F_INF, F_INF, -1.0f);
+                    s_ctin[w][lane] = -1.0f;
+                }
+                __syncwarp();
+                if(act) {
+                    unsigned in_mask = 0u, band_mask = 0u;
+    #pragma unroll
+                    for(int k = 0; k < 32; ++k) {
+                        const float4 b = s_cf[w][k];
+                        const float dx = ax - b.x, dy = ay - b.y, dz = az - b.z;
+                        const float r2f = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                        const float to = IJ ? fmaxf(Ti_out, b.w) : Ti_out;
+                        const float ti = IJ ? fmaxf(Ti_in, s_ctin[w][k]) : Ti_in;
+                        const bool inside = r2f < ti;
+                        const bool band = !inside && !(r2f >= to);  // NaN offsets land here
+                        in_mask |= (unsigned)inside << k;
+                        band_mask |= (unsigned)band << k;
+                    }
+                    while(band_mask) {
+                        const int k = __ffs(band_mask) - 1;
+                        band_mask &= band_mask - 1u;
+                        const int q = s_cid[w][k];
+                        const double4 pj = s_cpos[w][k];
+                        double h = hi;
+                        if(IJ) h = hi < pj.w ? pj.w : hi;
+                        const Vec3d r = rij(P, xi, yi, zi, pj.x, pj.y, pj.z);
+                        const double r2 = abs2x(r);
+                        if(!(r2 < h * h)) continue;
+                        const double hs = h - delta;
+                        bool take = hs > 0.0 && r2 < hs * hs;
+                        if(!take) {
+                            // on the radius: replay the reference's box tests up the path
+                            take = true;
+                            int A = __ldg(&T.leaf_of[q]);
+                            for(int up_ = 0; A >= 0 && up_ < 64; ++up_) {
+                                if(!box_pass<IJ>(P, T, A, xi, yi, zi, hi)) {
+                                    take = false;
+                                    break;
+                                }
+                                A = A == 0 ? -1 : T.parent[A];
+                            }
+                        }
+                        if(take) in_mask |= 1u << k;
+                    }
+                    while(in_mask) {
+                        const int k = __ffs(in_mask) - 1;
+                        in_mask &= in_mask - 1u;
+                        if(cnt < cap) list[row + cnt] = s_cid[w][k];
                         ++cnt;
                     }
                 }
+                __syncwarp();
             }
-        }
-        __syncwarp();
-    };
+        };
 
-    const int nnodes = *T.nnodes;
-    int steps = 0;
-    while(sp > 0) {
-        if(++steps > nnodes + 1) {  // each node is pushed at most once
-            overflow = true;
-            break;
-        }
-        const int m = sp < 32 ? sp : 32;
-        const int nd = lane < m ? s_stack[w][sp - 1 - lane] : -1;
-        __syncwarp();
-        sp -= m;
-        bool pass = false, leaf = false;
-        int4 c0 = make_int4(-1, -1, -1, -1), c1 = c0;
-        if(nd >= 0) {
-            const int4 lk = __ldg(&T.link[nd]);
-            const double4 g = ldg4(&T.geo[nd]);
-            leaf = (lk.w >> 8) != 0;
-            double hh = hmax;
-            if(IJ) hh = fmax(hmax, __ldg(&T.ksize[nd]));
-            const double reach = (g.w * 0.5 + hh) * (1.0 + 1e-10) + delta;
-            const double cc[3] = {g.x, g.y, g.z};
-            pass = true;
-            for(int k = 0; k < 3; ++k) {
-                double gap = interval_gap(cc[k], lo[k], up[k]);
-                if(P.periodic) {
-                    gap = fmin(gap, interval_gap(cc[k] + P.range[k], lo[k], up[k]));
-                    gap = fmin(gap, interval_gap(cc[k] - P.range[k], lo[k], up[k]));
-                }
-                pass = pass && gap <= reach;
+        const int nnodes = *T.nnodes;
+        int steps = 0;
+        while(sp > 0) {
+            if(++steps > nnodes + 1) {  // each node is pushed at most once
+                overflow = true;
+                break;
             }
-            if(pass && !leaf) {
-                const int4* cp = reinterpret_cast<const int4*>(T.child + (size_t)nd * 8);
-                c0 = __ldg(cp);
-                c1 = __ldg(cp + 1);
-            }
-        }
-        // push children of passing internal nodes (order within a step is free)
-        const int kids[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-        int nk = 0;
-        for(int k = 0; k < 8; ++k) nk += kids[k] >= 0 ? 1 : 0;
-        int incl = nk;
-        for(int o = 1; o < 32; o <<= 1) {
-            const int u = __shfl_up_sync(FULL_MASK, incl, o);
-            if(lane >= o) incl += u;
-        }
-        const int total = __shfl_sync(FULL_MASK, incl, 31);
-        if(sp + total > GW_STACK) {
-            overflow = true;
-            break;
-        }
-        int pos = sp + incl - nk;
-        for(int k = 0; k < 8; ++k) {
-            if(kids[k] >= 0) s_stack[w][pos++] = kids[k];
-        }
-        sp += total;
-        // queue passing leaves
-        const unsigned lb = __ballot_sync(FULL_MASK, pass && leaf);
-        if(pass && leaf) s_queue[w][nq + __popc(lb & ((1u << lane) - 1u))] = nd;
-        nq += __popc(lb);
-        __syncwarp();
-        if(nq >= 32) {
-            process(32);
-            nq -= 32;
-            if(lane < nq) s_queue[w][lane] = s_queue[w][32 + lane];
+            const int m = sp < 32 ? sp : 32;
+            const int nd = lane < m ? s_stack[w][sp - 1 - lane] : -1;
             __syncwarp();
+            sp -= m;
+            bool pass = false, leaf = false;
+            int4 c0 = make_int4(-1, -1, -1, -1), c1 = c0;
+            if(nd >= 0) {
+                const int4 lk = __ldg(&T.link[nd]);
+                const double4 g = ldg4(&T.geo[nd]);
+                leaf = (lk.w >> 8) != 0;
+                double hh = bh;
+                if(IJ) hh = fmax(bh, __ldg(&T.ksize[nd]));
+                const double reach = (g.w * 0.5 + hh) * (1.0 + 1e-10) + delta;
+                const double cc[3] = {g.x, g.y, g.z};
+                pass = true;
+                for(int k = 0; k < 3; ++k) {
+                    double gap = interval_gap(cc[k], blo[k], bup[k]);
+                    if(P.periodic) {
+                        gap = fmin(gap, interval_gap(cc[k] + P.range[k], blo[k], bup[k]));
+                        gap = fmin(gap, interval_gap(cc[k] - P.range[k], blo[k], bup[k]));
+                    }
+                    pass = pass && gap <= reach;
+                }
+                if(pass && !leaf) {
+                    // queue every particle of a small node, or of a node whose
+                    // box lies inside the group's search box (all its leaves
+                    // would pass), instead of descending: the candidate set only
+                    // grows, and the per-pair classification decides
+                    bool whole = lk.y - lk.x <= GW_WHOLE;
+                    if(!whole) {
+                        const double he = g.w * 0.5;
+                        whole = true;
+                        for(int k = 0; k < 3; ++k) whole = whole && cc[k] - he >= blo[k] - bh && cc[k] + he <= bup[k] + bh;
+                    }
+                    if(whole) {
+                        leaf = true;
+                    } else {
+                        const int4* cp = reinterpret_cast<const int4*>(T.child + (size_t)nd * 8);
+                        c0 = __ldg(cp);
+                        c1 = __ldg(cp + 1);
+                    }
+                }
+            }
+            // push children of passing internal nodes (order within a step is free)
+            const int kids[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+            int nk = 0;
+            for(int k = 0; k < 8; ++k) nk += kids[k] >= 0 ? 1 : 0;
+            int incl = nk;
+            for(int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(FULL_MASK, incl, o);
+                if(lane >= o) incl += u;
+            }
+            const int total = __shfl_sync(FULL_MASK, incl, 31);
+            if(sp + total > GW_STACK) {
+                overflow = true;
+                break;
+            }
+            int pos = sp + incl - nk;
+            for(int k = 0; k < 8; ++k) {
+                if(kids[k] >= 0) s_stack[w][pos++] = kids[k];
+            }
+            sp += total;
+            // queue passing leaves
+            const unsigned lb = __ballot_sync(FULL_MASK, pass && leaf);
+            if(pass && leaf) s_queue[w][nq + __popc(lb & ((1u << lane) - 1u))] = nd;
+            nq += __popc(lb);
+            __syncwarp();
+            if(nq >= 32) {
+                process(32);
+                nq -= 32;
+                if(lane < nq) s_queue[w][lane] = s_queue[w][32 + lane];
+                __syncwarp();
+            }
         }
+        if(!overflow && nq > 0) process(nq);
     }
-    if(!overflow && nq > 0) process(nq);
     if(overflow) {
         if(lane == 0) st->guard = 2;
         return;
