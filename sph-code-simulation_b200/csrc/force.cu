@@ -173,8 +173,15 @@ __device__ void riemann_iterative(const double* L, const double* R, double gamma
 
 // MODE: 0 = force (optionally harvesting pair states), 1 = GSPH features of
 // the learned guess only (no force written), 2 = force with the learned guess.
+// Minimum resident blocks per SM (caps registers; measured on B200).
+template <typename T, int TYPE>
+constexpr int force_min_blocks()
+{
+    return (sizeof(T) == sizeof(float) || TYPE == SPHGPU_GSPH) ? 4 : 3;
+}
+
 template <typename T, int G, int TYPE, int MODE>
-__global__ void __launch_bounds__(FBLK) k_force(DevParams P, DevState S, int n, const int* __restrict__ list,
+__global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(DevParams P, DevState S, int n, const int* __restrict__ list,
                                                 const int* __restrict__ count, int cap, const double* __restrict__ dtp,
                                                 DevStatus* __restrict__ st, MlpPairs mp, Harvest hv)
 {

@@ -39,8 +39,27 @@ __device__ __forceinline__ double exact_r(const DevParams& P, double xi, double 
     return sqrt(abs2x(d));
 }
 
+// r = |r_ij| with the reference's rounding (sqrt of the unfused r^2), or -1
+// when r^2 exceeds h^2 (1 + 2^-40): then the correctly rounded sqrt is above
+// h, so r < h is false and the square root is skipped.
+__device__ __forceinline__ double r_within(const DevParams& P, double xi, double yi, double zi, double4 pj, double h,
+                                           Vec3d& d)
+{
+    d = rij(P, xi, yi, zi, pj.x, pj.y, pj.z);
+    const double r2 = abs2x(d);
+    if(r2 > h * h * (1.0 + 0x1p-40)) return -1.0;
+    return sqrt(r2);
+}
+
+// Minimum resident blocks per SM (caps registers; measured on B200).
+template <typename T, int TYPE>
+constexpr int pre_min_blocks()
+{
+    return (sizeof(T) == sizeof(float) && TYPE != SPHGPU_GSPH) ? 4 : 3;
+}
+
 template <typename T, int G, int TYPE>
-__global__ void __launch_bounds__(PBLK) k_pre(DevParams P, DevState S, int n, const int* __restrict__ list,
+__global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevParams P, DevState S, int n, const int* __restrict__ list,
                                               const int* __restrict__ count, int cap, const double* __restrict__ dtp,
                                               double* __restrict__ hvs, DevStatus* __restrict__ st)
 {
@@ -77,8 +96,8 @@ __global__ void __launch_bounds__(PBLK) k_pre(DevParams P, DevState S, int n, co
                 for(int k = lane; k < cnt; k += G) {
                     const double4 pj = S.pos[li[k]];
                     Vec3d dv;
-                    const double r = exact_r(P, pi.x, pi.y, pi.z, pj, dv);
-                    if(r < h) {
+                    const double r = r_within(P, pi.x, pi.y, pi.z, pj, h, dv);
+                    if(r >= 0.0 && r < h) {
                         const T w = kh.w((T)r);
                         const T dh = kh.dhw((T)r);
                         if(disph) {
@@ -119,8 +138,8 @@ __global__ void __launch_bounds__(PBLK) k_pre(DevParams P, DevState S, int n, co
             const int j = li[k];
             const double4 pj = S.pos[j];
             Vec3d dv;
-            const double r = exact_r(P, pi.x, pi.y, pi.z, pj, dv);
-            if(!(r < h)) continue;
+            const double r = r_within(P, pi.x, pi.y, pi.z, pj, h, dv);
+            if(!(r >= 0.0 && r < h)) continue;
             ++nn;
             const double4 vj = S.vel[j];
             const double4 tj = S.thermo[j];
