@@ -308,12 +308,12 @@ def run_gpu(args, rank: int, world: int, local: int):
                 "algorithmic_bytes_per_launch": algo, "launch_ms": round(per_launch_ms, 4),
                 "accounting": unit_note}
     prof = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(prof):
+    if os.path.exists(prof) and not args.particles:
         try:
-            tr = json.load(open(prof)).get(dom)
+            tr = json.load(open(prof)).get(args.workload, {}).get(dom)
             if tr:
                 roofline["traffic"] = tr
-        except Exception:
+        except (OSError, ValueError):
             pass
     sim.close()
 
