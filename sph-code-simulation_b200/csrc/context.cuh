@@ -61,6 +61,7 @@ struct sphgpu_ctx {
     float* d_mlp_master = nullptr;    // FP32 master parameters + Adam moments
     uint4* d_mlp_feat = nullptr;      // per pair slot: scaled features (bf16)
     float* d_mlp_y = nullptr;         // per pair slot: network output
+    unsigned long long* d_mlp_rows = nullptr;  // compacted feature rows of the current call
     int64_t mlp_slots = 0;
     bool have_mlp = false;
     std::vector<float> mlp_master;

@@ -89,13 +89,36 @@ __device__ __forceinline__ double vl_ustar(double p, double ul, double pl, doubl
     return 0.5 * (usl + usr);
 }
 
+// Screen of the learned start: one Newton step from the reference's
+// linearised guess (src/gsph/g_fluid_force.cpp:244-246).  Returns the relative
+// change and the stepped pressure.  Not inlined, so the feature pass and the
+// force pass take the same decision for the same pair.
+__device__ __noinline__ double learned_screen(double ul, double pl, double vl, double cl, double ur, double pr,
+                                              double vr, double cr, double g1, double g2, double& q1)
+{
+    double q0 = pr - pl - cr * (ur - ul);
+    q0 = fmax(pl + q0 * cl / (cl + cr), 1e-25);
+    q1 = vl_newton_step<double>(q0, ul, pl, vl, cl, ur, pr, vr, cr, g1, g2);
+    return fabs(q1 - q0) / q1;
+}
+
+__device__ __forceinline__ bool learned_needed(const double* L, const double* R, double gamma)
+{
+    if(!(L[1] > 0.0 && R[1] > 0.0 && L[2] > 0.0 && R[2] > 0.0)) return false;
+    const double g2 = 1.0 + gamma, g1 = 0.5 * g2 / gamma;
+    const double cl = sqrt(gamma * L[2] * L[1]), cr = sqrt(gamma * R[2] * R[1]);
+    double q1;
+    return !(learned_screen(L[0], L[2], 1.0 / L[1], cl, R[0], R[2], 1.0 / R[1], cr, g1, g2, q1) < 1e-2);
+}
+
 // Iterative solver (src/gsph/g_fluid_force.cpp:209-304).  Plain form: FP64
 // throughout.  Mixed form: iterations in T = float, then one FP64 Newton step
-// and the FP64 u*.  With `guess` > 0 (learned form) Newton starts from the
-// guess, runs at most `budget` iterations to a 1e-10 relative change (the
-// last checked in FP64) and falls back to the plain start on failure.
+// and the FP64 u*.  With `learned` set, Newton starts from the screened start
+// (below; y = the network's log(p_star / p_L), read only when the screen
+// rejects the linearised start), runs at most `budget` iterations to a 1e-10
+// relative change (in FP64) and falls back to the plain start on failure.
 template <typename T>
-__device__ void riemann_iterative(const double* L, const double* R, double gamma, double guess, int budget,
+__device__ void riemann_iterative(const double* L, const double* R, double gamma, bool learned, float y, int budget,
                                   double& pstar, double& vstar, int& iters, int& fallback)
 {
     const double ul = L[0], rhol = L[1], pl = L[2];
@@ -113,7 +136,7 @@ __device__ void riemann_iterative(const double* L, const double* R, double gamma
     const double cl = sqrt(gamma * pl * rhol);
     const double cr = sqrt(gamma * pr * rhor);
     double p;
-    if(guess > 0.0) {
+    if(learned) {
         // Learned start.  Screen first with one Newton step from the
         // reference's linearised guess: when that step moves p by less than
         // 1 % the linearised start is already in Newton's quadratic range
@@ -121,12 +144,11 @@ __device__ void riemann_iterative(const double* L, const double* R, double gamma
         // otherwise Newton restarts from the network's guess.  Either way
         // Newton runs to a 1e-10 relative change within `budget` iterations,
         // else the reference's solver takes over.
-        double q0 = pr - pl - cr * (ur - ul);
-        q0 = fmax(pl + q0 * cl / (cl + cr), 1e-25);
-        double q1 = vl_newton_step<double>(q0, ul, pl, vl, cl, ur, pr, vr, cr, g1, g2);
+        double q1;
+        const double ch = learned_screen(ul, pl, vl, cl, ur, pr, vr, cr, g1, g2, q1);
         iters = 1;
-        const double ch = fabs(q1 - q0) / q1;
-        p = ch < 1e-2 ? q1 : guess;
+        const double guess = pl * exp((double)y);
+        p = (ch < 1e-2 || !(guess > 0.0 && guess < 1e300)) ? q1 : guess;
         bool ok = ch < 1e-10;
         for(int it = 0; !ok && it < budget; ++it) {
             const double pold = p;
@@ -287,25 +309,23 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
                     Lst[3] = tj.w;
                 }
                 if(MODE == 1) {
-                    float x[MLP_IN];
-                    const bool ok = Lst[1] > 0.0 && Rst[1] > 0.0 && Lst[2] > 0.0 && Rst[2] > 0.0;
-                    if(ok) mlp_features(Lst, Rst, gamma, x);
-                    uint4 v;
-                    v.x = ok ? pack_bf16x2(x[0], x[1]) : 0u;
-                    v.y = ok ? pack_bf16x2(x[2], x[3]) : 0u;
-                    v.z = ok ? pack_bf16x2(x[4], 0.f) : 0u;
-                    v.w = 0u;
-                    mp.feat[(size_t)i * cap + k] = v;
+                    // features only for the pairs whose linearised start the
+                    // screen rejects, compacted, with the pair slot alongside
+                    if(learned_needed(Lst, Rst, gamma)) {
+                        float x[MLP_IN];
+                        mlp_features(Lst, Rst, gamma, x);
+                        const unsigned long long row = atomicAdd(mp.rows, 1ull);
+                        mp.feat[row] = make_uint4(pack_bf16x2(x[0], x[1]), pack_bf16x2(x[2], x[3]),
+                                                  pack_bf16x2(x[4], 0.f), (unsigned)((size_t)i * cap + k));
+                    }
                     continue;
                 }
                 double pstar, vstar;
                 if(P.riemann == SPHGPU_RIEMANN_ITERATIVE) {
-                    double guess = -1.0;
-                    if(MODE == 2 && Lst[1] > 0.0 && Rst[1] > 0.0 && Lst[2] > 0.0 && Rst[2] > 0.0) {
-                        guess = Lst[2] * exp((double)mp.y[(size_t)i * cap + k]);
-                    }
                     int it = 0, fb = 0;
-                    riemann_iterative<T>(Lst, Rst, gamma, guess, P.mlp_max_newton, pstar, vstar, it, fb);
+                    const bool learned = MODE == 2 && Lst[1] > 0.0 && Rst[1] > 0.0 && Lst[2] > 0.0 && Rst[2] > 0.0;
+                    riemann_iterative<T>(Lst, Rst, gamma, learned, learned ? mp.y[(size_t)i * cap + k] : 0.f,
+                                         P.mlp_max_newton, pstar, vstar, it, fb);
                     ++solves;
                     iters += it;
                     fallbacks += fb;
@@ -453,9 +473,9 @@ __global__ void k_riemann_batch(const double* __restrict__ st, long long n, int 
     double p = 0.0, v = 0.0;
     int it = 0, f = 0;
     if(mode == 0) {
-        riemann_iterative<double>(L, R, gamma, -1.0, budget, p, v, it, f);
+        riemann_iterative<double>(L, R, gamma, false, 0.f, budget, p, v, it, f);
     } else if(mode == 1) {
-        riemann_iterative<double>(L, R, gamma, L[2] * exp((double)y[r]), budget, p, v, it, f);
+        riemann_iterative<double>(L, R, gamma, true, y[r], budget, p, v, it, f);
     } else {
         // plain start, Newton to a relative change of 1e-13 (mode 2, labels)
         // or 1e-10 (mode 3, the learned path's target accuracy)
@@ -491,10 +511,11 @@ int fluid_force(sphgpu_ctx* c)
     if(rc_walk < 0) return rc_walk;
     stage_begin(c, SPHGPU_T_FORCE);
     Harvest hv{c->d_harvest, c->d_harvest_count, c->harvest_cap, c->harvest_mod, 0u};
-    MlpPairs mp{nullptr, nullptr};
+    MlpPairs mp{nullptr, nullptr, nullptr};
     int launches = 1;
     if(learned) {
         const int64_t slots = (int64_t)c->n * c->pcap;
+        if(slots > 0xFFFFFFFFLL) return fail(c, SPHGPU_ERR_ARG, "learned guess: more than 2^32 pair slots");
         if(slots > c->mlp_slots) {
             if(c->d_mlp_feat) cudaFree(c->d_mlp_feat);
             if(c->d_mlp_y) cudaFree(c->d_mlp_y);
@@ -504,11 +525,14 @@ int fluid_force(sphgpu_ctx* c)
             SPHGPU_CUDA(c, cudaMalloc(&c->d_mlp_y, sizeof(float) * (size_t)slots));
             c->mlp_slots = slots;
         }
+        if(!c->d_mlp_rows) SPHGPU_CUDA(c, cudaMalloc(&c->d_mlp_rows, sizeof(unsigned long long)));
+        SPHGPU_CUDA(c, cudaMemsetAsync(c->d_mlp_rows, 0, sizeof(unsigned long long), c->stream));
         mp.feat = c->d_mlp_feat;
         mp.y = c->d_mlp_y;
+        mp.rows = c->d_mlp_rows;
         if(c->prm.precision == SPHGPU_MIXED) launch_force<float, 1>(c, mp, hv);
         else launch_force<double, 1>(c, mp, hv);
-        const int rc = mlp_infer_pairs(c, c->d_pcount, c->n, (int)c->pcap);
+        const int rc = mlp_infer_pairs(c, c->d_mlp_rows, slots);
         if(rc < 0) return rc;
         if(c->prm.precision == SPHGPU_MIXED) launch_force<float, 2>(c, mp, hv);
         else launch_force<double, 2>(c, mp, hv);

@@ -64,11 +64,13 @@ __device__ __forceinline__ void mlp_features(const double* L, const double* R, d
     x[4] = (float)((gamma - 1.5) * 4.0);
 }
 
-// Pair-list-aligned buffers of the learned path: per pair slot i*cap + k the
-// scaled features (8 bf16, 5 used) and the network output log(p_star / p_L).
+// Buffers of the learned path: compacted feature rows (8 bf16, 5 used; .w =
+// the pair slot i*cap + k) for the pairs the screen sends to the network, the
+// row count, and per pair slot the network output log(p_star / p_L).
 struct MlpPairs {
     uint4* feat;
     const float* y;
+    unsigned long long* rows;
 };
 
 // Sampled pair states written by the plain solver (training data): records
@@ -81,7 +83,7 @@ struct Harvest {
     unsigned salt;
 };
 // Launchers (mlp.cu).
-int mlp_infer_pairs(sphgpu_ctx* c, const int* count, int n, int cap);
+int mlp_infer_pairs(sphgpu_ctx* c, const unsigned long long* d_rows, long long max_rows);
 int mlp_predict_states(sphgpu_ctx* c, const double* d_states, long long n, float* d_y);
 
 __device__ __forceinline__ unsigned pack_bf16x2(float lo, float hi)
