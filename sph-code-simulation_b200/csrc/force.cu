@@ -431,7 +431,7 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
     }
 }
 
-constexpr int GROUP = 8;
+constexpr int GROUP = 4;
 
 unsigned force_grid(int n)
 {

@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(PBLK) k_initial_density(DevParams P, DevState 
     }
 }
 
-constexpr int GROUP = 8;
+constexpr int GROUP = 4;
 
 unsigned pre_grid(int n)
 {
