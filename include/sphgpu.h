@@ -131,6 +131,7 @@ typedef struct sphgpu_counters {
     int64_t walk_group_warps;      /* warps walked as one group of 32        */
     int64_t walk_split_warps;      /* warps walked as several sub-groups     */
     int64_t walk_fallbacks;        /* group walks redone per lane (overflow) */
+    int64_t mlp_guesses;           /* pairs whose start came from the network */
 } sphgpu_counters;
 
 /* Stage timers (ms, summed since the last reset; CUDA events on the

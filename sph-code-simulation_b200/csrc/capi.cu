@@ -684,6 +684,7 @@ int sphgpu_get_counters(sphgpu_ctx* c, sphgpu_counters* o)
     o->walk_group_warps = (int64_t)c->h_status.walk_group_warps;
     o->walk_split_warps = (int64_t)c->h_status.walk_split_warps;
     o->walk_fallbacks = c->walk_fallbacks;
+    o->mlp_guesses = (int64_t)c->h_status.mlp_guesses;
     return SPHGPU_OK;
 }
 

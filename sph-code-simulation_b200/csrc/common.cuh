@@ -85,6 +85,7 @@ struct DevStatus {
     unsigned long long riemann_fallbacks;
     unsigned long long walk_group_warps;   // warps that took the group walk
     unsigned long long walk_split_warps;   // warps walked as several sub-groups
+    unsigned long long mlp_guesses;        // pairs sent to the learned guess
 };
 
 // Read-only 32-byte load through the non-coherent path (two 16-byte halves).

@@ -315,6 +315,7 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
                         float x[MLP_IN];
                         mlp_features(Lst, Rst, gamma, x);
                         const unsigned long long row = atomicAdd(mp.rows, 1ull);
+                        atomicAdd(&st->mlp_guesses, 1ull);
                         mp.feat[row] = make_uint4(pack_bf16x2(x[0], x[1]), pack_bf16x2(x[2], x[3]),
                                                   pack_bf16x2(x[4], 0.f), (unsigned)((size_t)i * cap + k));
                     }

@@ -82,7 +82,7 @@ class Counters(C.Structure):
     _fields_ = [(n, C.c_int64) for n in (
         "newton_nonconverged", "riemann_solves", "riemann_iterations", "riemann_fallbacks",
         "gather_capacity", "max_gather", "max_pair", "node_count", "retries", "walk_group_warps",
-        "walk_split_warps", "walk_fallbacks")]
+        "walk_split_warps", "walk_fallbacks", "mlp_guesses")]
 
 
 _lib = None
