@@ -4,7 +4,7 @@
 // the reference's unmodified sources (src/bhtree.cpp, src/pre_interaction.cpp,
 // src/fluid_force.cpp, src/gravity_force.cpp, src/timestep.cpp,
 // src/simulation.cpp, src/exhaustive_search.cpp, src/disph/*.cpp,
-// src/gsph/*.cpp) by oracle/Makefile into oracle/_ref/libsphref.so (tree
+// src/gsph/*.cpp, src/gdisph/*.cpp) by oracle/Makefile into oracle/_ref/libsphref.so (tree
 // search) and oracle/_ref/libsphref_exh.so (-DEXHAUSTIVE_SEARCH).  It is the
 // checker the CPU restatement (oracle/sph_oracle.cpp) and the GPU path are
 // compared with, and the CPU baseline that bench.py --impl reference times.
@@ -34,6 +34,8 @@
 #include "disph/d_fluid_force.hpp"
 #include "gsph/g_pre_interaction.hpp"
 #include "gsph/g_fluid_force.hpp"
+#include "gdisph/gd_pre_interaction.hpp"
+#include "gdisph/gd_fluid_force.hpp"
 #include "exhaustive_search.hpp"
 #include "exception.hpp"
 
@@ -57,8 +59,9 @@ std::shared_ptr<SPHParameters> to_param(const sphgpu_params* p)
     std::memset(q.get(), 0, sizeof(SPHParameters));
     q->time.start = 0.0;
     q->time.end = 1.0;
-    q->type = p->sph_type == SPHGPU_DISPH ? SPHType::DISPH
-            : p->sph_type == SPHGPU_GSPH  ? SPHType::GSPH : SPHType::SSPH;
+    q->type = p->sph_type == SPHGPU_DISPH  ? SPHType::DISPH
+            : p->sph_type == SPHGPU_GSPH   ? SPHType::GSPH
+            : p->sph_type == SPHGPU_GDISPH ? SPHType::GDISPH : SPHType::SSPH;
     q->cfl.sound = p->cfl_sound;
     q->cfl.force = p->cfl_force;
     q->av.alpha = p->av_alpha;
@@ -210,6 +213,11 @@ void* ref_create(const sphgpu_params* p, int64_t n, const double* const* fields)
         c->fforce = std::make_shared<gsph::FluidForce>();
         std::vector<std::string> names(grad_names, grad_names + 5);
         c->sim->add_vector_array(names);
+    } else if(c->param->type == SPHType::GDISPH) {
+        c->pre = std::make_shared<gdisph::PreInteraction>();
+        c->fforce = std::make_shared<gdisph::FluidForce>();
+        std::vector<std::string> names(grad_names, grad_names + 5);
+        c->sim->add_vector_array(names);
     } else {
         c->pre = std::make_shared<PreInteraction>();
         c->fforce = std::make_shared<FluidForce>();
@@ -238,7 +246,7 @@ int ref_get(void* h, double* const* fields)
         }
         if(fields[SPHGPU_F_NEIGHBOR]) fields[SPHGPU_F_NEIGHBOR][i] = parts[i].neighbor;
     }
-    if(c->param->type == SPHType::GSPH) {
+    if(c->param->type == SPHType::GSPH || c->param->type == SPHType::GDISPH) {
         for(int g = 0; g < 5; ++g) {
             auto& arr = c->sim->get_vector_array(grad_names[g]);
             for(int d = 0; d < 3; ++d) {

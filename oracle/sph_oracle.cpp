@@ -579,8 +579,10 @@ struct Oracle {
     }
 
     // PreInteraction::calculation for ssph (src/pre_interaction.cpp:39-169),
-    // disph (src/disph/d_pre_interaction.cpp:21-162) and gsph
-    // (src/gsph/g_pre_interaction.cpp:27-144).
+    // disph (src/disph/d_pre_interaction.cpp:21-162), gsph
+    // (src/gsph/g_pre_interaction.cpp:27-144) and gdisph
+    // (src/gdisph/gd_pre_interaction.cpp:29-198: the disph smoothing length,
+    // density and pressure, the gsph gradients, its own AV switches).
     bool pre_interaction()
     {
         if(first_pre) {
@@ -588,7 +590,8 @@ struct Oracle {
             first_pre = false;
         }
         const int type = prm.sph_type;
-        const bool disph = type == SPHGPU_DISPH, gsph = type == SPHGPU_GSPH;
+        const bool gdisph = type == SPHGPU_GDISPH;
+        const bool disph = type == SPHGPU_DISPH || gdisph, gsph = type == SPHGPU_GSPH;
         const real ratio = prm.iterative_sml ? 1.2 : 1.0;
         const real gamma = prm.gamma;
         real hvs = std::numeric_limits<real>::max();
@@ -649,9 +652,9 @@ struct Oracle {
             const real hv = sml / vsig;
             if(hv < hvs) hvs = hv;
 
-            if(gsph) {
-                // MUSCL gradients (src/gsph/g_pre_interaction.cpp:112-136)
-                if(!prm.gsph_2nd_order) continue;
+            if((gsph || gdisph) && prm.gsph_2nd_order) {
+                // MUSCL gradients (src/gsph/g_pre_interaction.cpp:112-136,
+                // src/gdisph/gd_pre_interaction.cpp:119-139)
                 V3 dd{0, 0, 0}, du{0, 0, 0}, dv[3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
                 const real ui = s.f[SPHGPU_F_ENE][i];
                 for(int n = 0; n < nn; ++n) {
@@ -671,11 +674,13 @@ struct Oracle {
                 s.set_grad(1, i, (dd * ui + du) * (gamma - 1.0));
                 const real rinv = 1.0 / s.f[SPHGPU_F_DENS][i];
                 for(int k = 0; k < 3; ++k) s.set_grad(2 + k, i, dv[k] * rinv);
-                continue;
             }
+            if(gsph) continue;
 
             // artificial viscosity switches (src/pre_interaction.cpp:115-161,
-            // src/disph/d_pre_interaction.cpp:106-154)
+            // src/disph/d_pre_interaction.cpp:106-154; gdisph's Balsara switch
+            // weights by mass and normalises by density, its implicit alpha
+            // update weights by mass x energy, src/gdisph/gd_pre_interaction.cpp:141-195)
             const real hi = sml;
             real& alpha = s.f[SPHGPU_F_ALPHA][i];
             if(prm.use_balsara_switch) {
@@ -687,11 +692,12 @@ struct Oracle {
                     const real rr = norm(r);
                     const V3 dw = ker.dw(r, rr, hi);
                     const V3 vij = vi - s.vel(j);
-                    const real wgt = disph ? s.f[SPHGPU_F_MASS][j] * s.f[SPHGPU_F_ENE][j] : s.f[SPHGPU_F_MASS][j];
+                    const real wgt = (disph && !gdisph) ? s.f[SPHGPU_F_MASS][j] * s.f[SPHGPU_F_ENE][j]
+                                                        : s.f[SPHGPU_F_MASS][j];
                     divv -= wgt * dot(vij, dw);
                     rot = rot + cross(vij, dw) * wgt;
                 }
-                if(disph) {
+                if(disph && !gdisph) {
                     const real pinv = (gamma - 1.0) / s.f[SPHGPU_F_PRES][i];
                     divv *= pinv;
                     rot = rot * pinv;
@@ -755,6 +761,8 @@ struct Oracle {
 
     // FluidForce::calculation for ssph (src/fluid_force.cpp:26-86), disph
     // (src/disph/d_fluid_force.cpp:26-86), gsph (src/gsph/g_fluid_force.cpp:44-171)
+    // and gdisph (src/gdisph/gd_fluid_force.cpp:45-178: the gsph MUSCL states
+    // and HLL star pressure inside the disph pressure-energy terms)
     bool fluid_force()
     {
         const int type = prm.sph_type;
@@ -784,11 +792,12 @@ struct Oracle {
                 const real mj = s.f[SPHGPU_F_MASS][j];
                 const V3 dwi = ker.dw(r, rr, hi);
                 const V3 dwj = ker.dw(r, rr, hj);
-                if(type == SPHGPU_GSPH) {
+                real pstar = 0.0, vstar = 0.0;
+                V3 e{0, 0, 0};
+                if(type == SPHGPU_GSPH || type == SPHGPU_GDISPH) {
                     const real rinv = 1.0 / rr;
-                    const V3 e = r * rinv;
+                    e = r * rinv;
                     const real vei = dot(vi, e), vej = dot(vj, e);
-                    real pstar, vstar;
                     real L[4], R[4];
                     if(prm.gsph_2nd_order) {
                         const real di = 0.5 * (1.0 - s.f[SPHGPU_F_SOUND][i] * dt * rinv);
@@ -820,12 +829,14 @@ struct Oracle {
                         R[0] = vei; R[1] = rhoi; R[2] = Pi; R[3] = s.f[SPHGPU_F_SOUND][i];
                         L[0] = vej; L[1] = s.f[SPHGPU_F_DENS][j]; L[2] = s.f[SPHGPU_F_PRES][j]; L[3] = s.f[SPHGPU_F_SOUND][j];
                     }
-                    if(prm.riemann_solver == SPHGPU_RIEMANN_ITERATIVE) {
+                    if(type == SPHGPU_GSPH && prm.riemann_solver == SPHGPU_RIEMANN_ITERATIVE) {
                         iters += riemann_iterative(L, R, prm.gamma, pstar, vstar);
                         ++solves;
                     } else {
                         riemann_hll(L, R, pstar, vstar);
                     }
+                }
+                if(type == SPHGPU_GSPH) {
                     const V3 vij = e * vstar;
                     const real r2i = 1.0 / sqr(rhoi);
                     const real r2j = 1.0 / sqr(s.f[SPHGPU_F_DENS][j]);
@@ -848,6 +859,19 @@ struct Oracle {
                     const real upj = uj / s.f[SPHGPU_F_PRES][j];
                     acc = acc - (dwi * (mj * (g2up * uj * fij + 0.5 * pij)) + dwj * (mj * (g2u * upj * fji + 0.5 * pij)));
                     dene += mj * g2up * uj * fij * dot(vij, dwi) + 0.5 * mj * pij * dot(vij, dwij) + dac;
+                } else if(type == SPHGPU_GDISPH) {
+                    const real g2u = sqr(prm.gamma - 1.0) * ui;
+                    const real g2up = g2u / Pi;
+                    const real muinv = 1.0 / (mi * ui);
+                    const real uj = s.f[SPHGPU_F_ENE][j];
+                    const real Pj = s.f[SPHGPU_F_PRES][j];
+                    const real fij = 1.0 - gi / (mj * uj);
+                    const real fji = 1.0 - s.f[SPHGPU_F_GRADH][j] * muinv;
+                    const real upj = uj / Pj;
+                    const real psi = pstar / Pi, psj = pstar / Pj;
+                    acc = acc - (dwi * (mj * (g2up * uj * fij * psi + 0.5 * pij))
+                                 + dwj * (mj * (g2u * upj * fji * psj + 0.5 * pij)));
+                    dene += mj * g2up * uj * fij * psi * dot(vij, dwi) + 0.5 * mj * pij * dot(vij, dwij) + dac;
                 } else {
                     const real ppr = Pi / sqr(rhoi);
                     const real pj = s.f[SPHGPU_F_PRES][j] / sqr(s.f[SPHGPU_F_DENS][j]);

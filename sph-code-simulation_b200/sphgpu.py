@@ -25,7 +25,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsphgpu.so")
 
 # enums (include/sphgpu.h)
-SSPH, DISPH, GSPH = 0, 1, 2
+SSPH, DISPH, GSPH, GDISPH = 0, 1, 2, 3
 CUBIC_SPLINE, WENDLAND = 0, 1
 RIEMANN_HLL, RIEMANN_ITERATIVE = 0, 1
 FP64, MIXED = 0, 1
@@ -451,6 +451,11 @@ def config_params(name: str, **overrides) -> Params:
         p = default_params(sph_type=GSPH, kernel=CUBIC_SPLINE, neighbor_number=50, gsph_2nd_order=1,
                            riemann_solver=RIEMANN_ITERATIVE, gamma=1.4, periodic=1,
                            range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.05, 0.05))
+    elif name == "tube_gdisph":        # gdisph shock tube, MUSCL + HLL, cubic, K=50, Balsara, TD-AV, AC
+        p = default_params(sph_type=GDISPH, kernel=CUBIC_SPLINE, neighbor_number=50, gsph_2nd_order=1,
+                           riemann_solver=RIEMANN_HLL, gamma=1.4, periodic=1, use_balsara_switch=1,
+                           use_time_dependent_av=1, alpha_min=0.1, alpha_max=2.0, epsilon_av=0.2, av_alpha=1.0,
+                           use_ac=1, alpha_ac=1.0, range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.05, 0.05))
     elif name == "evrard_disph":       # disph + gravity sphere, Wendland, K=128, TD-AV, AC
         p = default_params(sph_type=DISPH, kernel=WENDLAND, neighbor_number=128, use_time_dependent_av=1,
                            alpha_min=0.1, alpha_max=2.0, epsilon_av=0.2, use_balsara_switch=1, use_ac=1,

@@ -17,7 +17,8 @@ oracle/_ref/libsphref*.so, driven by oracle/ref_harness.cpp):
                      printed 6 digits, then stores every 16th particle's printed
                      row, the recomputed full-precision values for the same
                      particles, and W0.
-  steps_<cfg>.npz    Small instances of the four benchmark workloads: the
+  steps_<cfg>.npz    Small instances of the benchmark workloads (and of the
+                     gdisph shock tube, first and second order): the
                      full particle state after Solver::initialize and after
                      each of two Solver::integrate steps, plus dt.
   lists_<cfg>.npz    Distance-sorted neighbour lists (CSR) from
@@ -60,6 +61,11 @@ SMALL = {
                       lambda: G.sample_shock_tube(0.025, ly=0.1)),
     "shear_disph": (lambda: G.config_params("shear_disph", neighbor_number=64),
                     lambda: G.sample_shear_layer(0.05, lz=0.125)),
+    "tube_gdisph": (lambda: G.config_params("tube_gdisph", range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.1, 0.1)),
+                    lambda: G.sample_shock_tube(0.025, ly=0.1)),
+    "tube_gdisph_1st": (lambda: G.config_params("tube_gdisph", gsph_2nd_order=0, use_balsara_switch=0,
+                                                range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.1, 0.1)),
+                        lambda: G.sample_shock_tube(0.025, ly=0.1)),
 }
 
 

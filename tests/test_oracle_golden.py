@@ -9,7 +9,8 @@ import pytest
 
 from conftest import golden, params_from_bytes
 
-SMALL = ["evrard_ssph", "evrard_disph", "tube_gsph", "tube_gsph_hll", "shear_disph"]
+SMALL = ["evrard_ssph", "evrard_disph", "tube_gsph", "tube_gsph_hll", "shear_disph", "tube_gdisph",
+         "tube_gdisph_1st"]
 
 
 def _fields_from_ic(g):
