@@ -291,7 +291,8 @@ __global__ void k_iota(int* __restrict__ id, int n)
 
 int check_params(const sphgpu_params* p, std::string& why)
 {
-    if(p->sph_type < SPHGPU_SSPH || p->sph_type > SPHGPU_GSPH) return why = "SPH type must be ssph, disph or gsph", -1;
+    if(p->sph_type < SPHGPU_SSPH || p->sph_type > SPHGPU_GDISPH)
+        return why = "SPH type must be ssph, disph, gsph or gdisph", -1;
     if(p->kernel != SPHGPU_CUBIC_SPLINE && p->kernel != SPHGPU_WENDLAND) return why = "kernel is unknown.", -1;
     if(p->neighbor_number <= 0) return why = "neighborNumber must be positive", -1;
     if(p->max_tree_level < 1 || p->max_tree_level > 21) return why = "maxTreeLevel must be in 1..21", -1;

@@ -1,9 +1,11 @@
-// force.cu — FluidForce::calculation for ssph, disph and gsph.
+// force.cu — FluidForce::calculation for ssph, disph, gsph and gdisph.
 //
 // Reference: src/fluid_force.cpp:26-116 (ssph pair force, Monaghan-97
 // artificial viscosity, artificial conductivity), src/disph/d_fluid_force.cpp:26-86
 // (Hopkins-2013 pressure-energy force), src/gsph/g_fluid_force.cpp:32-304
-// (van Leer limiter, MUSCL reconstruction, HLL and iterative Riemann solvers).
+// (van Leer limiter, MUSCL reconstruction, HLL and iterative Riemann solvers),
+// src/gdisph/gd_fluid_force.cpp:45-228 (gdisph: the MUSCL states' HLL star
+// pressure inside the disph pressure-energy terms).
 //
 // Gather form, no atomics: a group of G lanes owns particle i and strides over
 // its symmetric list (the is_ij tree walk), skipping pairs with
@@ -199,7 +201,7 @@ __device__ void riemann_iterative(const double* L, const double* R, double gamma
 template <typename T, int TYPE>
 constexpr int force_min_blocks()
 {
-    return (sizeof(T) == sizeof(float) || TYPE == SPHGPU_GSPH) ? 4 : 3;
+    return (sizeof(T) == sizeof(float) || TYPE == SPHGPU_GSPH || TYPE == SPHGPU_GDISPH) ? 4 : 3;
 }
 
 template <typename T, int G, int TYPE, int MODE>
@@ -226,7 +228,7 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
         const double4 si = valid ? S.visc[i] : make_double4(0, 0, 1, 0);
         const double hi = vi.w;
         double4 gi0 = make_double4(0, 0, 0, 0), gi1 = gi0, gi2 = gi0, gi3 = gi0;
-        if(TYPE == SPHGPU_GSPH && P.gsph2 && valid) {
+        if((TYPE == SPHGPU_GSPH || TYPE == SPHGPU_GDISPH) && P.gsph2 && valid) {
             gi0 = S.grad[i];
             gi1 = S.grad[(size_t)n + i];
             gi2 = S.grad[2 * (size_t)n + i];
@@ -261,7 +263,11 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
             const V3<T> dwj{rv.x * cj_, rv.y * cj_, rv.z * cj_};
             const T mj = (T)pj.w;
             const T rhoj = (T)tj.x, Pj = (T)tj.y, uj = (T)tj.z, cj = (T)tj.w;
-            if(TYPE == SPHGPU_GSPH) {
+            // gdisph: the HLL star pressure of the MUSCL states scales the disph
+            // pressure terms below by p_star / P_i and p_star / P_j
+            // (src/gdisph/gd_fluid_force.cpp:95-178)
+            T psi = T(1), psj = T(1);
+            if(TYPE == SPHGPU_GSPH || TYPE == SPHGPU_GDISPH) {
                 const double rinv = 1.0 / r;
                 const double ex = d.x * rinv, ey = d.y * rinv, ez = d.z * rinv;
                 const double vei = vi.x * ex + vi.y * ey + vi.z * ez;
@@ -308,70 +314,86 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
                     Lst[2] = tj.y;
                     Lst[3] = tj.w;
                 }
-                if(MODE == 1) {
-                    // features only for the pairs whose linearised start the
-                    // screen rejects, compacted, with the pair slot alongside
-                    if(learned_needed(Lst, Rst, gamma)) {
-                        float x[MLP_IN];
-                        mlp_features(Lst, Rst, gamma, x);
-                        const unsigned long long row = atomicAdd(mp.rows, 1ull);
-                        atomicAdd(&st->mlp_guesses, 1ull);
-                        mp.feat[row] = make_uint4(pack_bf16x2(x[0], x[1]), pack_bf16x2(x[2], x[3]),
-                                                  pack_bf16x2(x[4], 0.f), (unsigned)((size_t)i * cap + k));
+                if(TYPE == SPHGPU_GDISPH) {
+                    double pg, vg;
+                    if(sizeof(T) == sizeof(double)) {
+                        riemann_hll<double>(Lst, Rst, pg, vg);
+                    } else {
+                        const float Lf[4] = {(float)Lst[0], (float)Lst[1], (float)Lst[2], (float)Lst[3]};
+                        const float Rf[4] = {(float)Rst[0], (float)Rst[1], (float)Rst[2], (float)Rst[3]};
+                        float ps, vs;
+                        riemann_hll<float>(Lf, Rf, ps, vs);
+                        pg = ps;
                     }
-                    continue;
+                    psi = (T)pg / Pi;
+                    psj = (T)pg / Pj;
                 }
-                double pstar, vstar;
-                if(P.riemann == SPHGPU_RIEMANN_ITERATIVE) {
-                    int it = 0, fb = 0;
-                    const bool learned = MODE == 2 && Lst[1] > 0.0 && Rst[1] > 0.0 && Lst[2] > 0.0 && Rst[2] > 0.0;
-                    riemann_iterative<T>(Lst, Rst, gamma, learned, learned ? mp.y[(size_t)i * cap + k] : 0.f,
-                                         P.mlp_max_newton, pstar, vstar, it, fb);
-                    ++solves;
-                    iters += it;
-                    fallbacks += fb;
-                    if(MODE == 0 && hv.mod) {
-                        unsigned hsh = (unsigned)i * 0x9E3779B1u ^ (unsigned)k * 0x85EBCA77u ^ hv.salt;
-                        hsh ^= hsh >> 15;
-                        hsh *= 0x2C1B3C6Du;
-                        hsh ^= hsh >> 12;
-                        if(hsh % hv.mod == 0) {
-                            const unsigned long long slot = atomicAdd(hv.count, 1ull);
-                            if((long long)slot < hv.cap) {
-                                double* o = hv.out + 8 * slot;
-                                o[0] = Lst[0];
-                                o[1] = Lst[1];
-                                o[2] = Lst[2];
-                                o[3] = Rst[0];
-                                o[4] = Rst[1];
-                                o[5] = Rst[2];
-                                o[6] = gamma;
-                                o[7] = pstar;
+                if constexpr(TYPE == SPHGPU_GSPH) {
+                    if(MODE == 1) {
+                        // features only for the pairs whose linearised start the
+                        // screen rejects, compacted, with the pair slot alongside
+                        if(learned_needed(Lst, Rst, gamma)) {
+                            float x[MLP_IN];
+                            mlp_features(Lst, Rst, gamma, x);
+                            const unsigned long long row = atomicAdd(mp.rows, 1ull);
+                            atomicAdd(&st->mlp_guesses, 1ull);
+                            mp.feat[row] = make_uint4(pack_bf16x2(x[0], x[1]), pack_bf16x2(x[2], x[3]),
+                                                      pack_bf16x2(x[4], 0.f), (unsigned)((size_t)i * cap + k));
+                        }
+                        continue;
+                    }
+                    double pstar, vstar;
+                    if(P.riemann == SPHGPU_RIEMANN_ITERATIVE) {
+                        int it = 0, fb = 0;
+                        const bool learned = MODE == 2 && Lst[1] > 0.0 && Rst[1] > 0.0 && Lst[2] > 0.0 && Rst[2] > 0.0;
+                        riemann_iterative<T>(Lst, Rst, gamma, learned, learned ? mp.y[(size_t)i * cap + k] : 0.f,
+                                             P.mlp_max_newton, pstar, vstar, it, fb);
+                        ++solves;
+                        iters += it;
+                        fallbacks += fb;
+                        if(MODE == 0 && hv.mod) {
+                            unsigned hsh = (unsigned)i * 0x9E3779B1u ^ (unsigned)k * 0x85EBCA77u ^ hv.salt;
+                            hsh ^= hsh >> 15;
+                            hsh *= 0x2C1B3C6Du;
+                            hsh ^= hsh >> 12;
+                            if(hsh % hv.mod == 0) {
+                                const unsigned long long slot = atomicAdd(hv.count, 1ull);
+                                if((long long)slot < hv.cap) {
+                                    double* o = hv.out + 8 * slot;
+                                    o[0] = Lst[0];
+                                    o[1] = Lst[1];
+                                    o[2] = Lst[2];
+                                    o[3] = Rst[0];
+                                    o[4] = Rst[1];
+                                    o[5] = Rst[2];
+                                    o[6] = gamma;
+                                    o[7] = pstar;
+                                }
                             }
                         }
+                    } else if(sizeof(T) == sizeof(double)) {
+                        riemann_hll<double>(Lst, Rst, pstar, vstar);
+                    } else {
+                        const float Lf[4] = {(float)Lst[0], (float)Lst[1], (float)Lst[2], (float)Lst[3]};
+                        const float Rf[4] = {(float)Rst[0], (float)Rst[1], (float)Rst[2], (float)Rst[3]};
+                        float ps, vs;
+                        riemann_hll<float>(Lf, Rf, ps, vs);
+                        pstar = ps;
+                        vstar = vs;
                     }
-                } else if(sizeof(T) == sizeof(double)) {
-                    riemann_hll<double>(Lst, Rst, pstar, vstar);
-                } else {
-                    const float Lf[4] = {(float)Lst[0], (float)Lst[1], (float)Lst[2], (float)Lst[3]};
-                    const float Rf[4] = {(float)Rst[0], (float)Rst[1], (float)Rst[2], (float)Rst[3]};
-                    float ps, vs;
-                    riemann_hll<float>(Lf, Rf, ps, vs);
-                    pstar = ps;
-                    vstar = vs;
+                    // f = dw_i m_j p* / rho_i^2 + dw_j m_j p* / rho_j^2 (src/gsph/g_fluid_force.cpp:158-165)
+                    const T ps = (T)pstar;
+                    const T fi = mj * ps * r2i;
+                    const T fj = mj * ps * (T(1) / (rhoj * rhoj));
+                    const double fx = (double)(dwi.x * fi + dwj.x * fj);
+                    const double fy = (double)(dwi.y * fi + dwj.y * fj);
+                    const double fz = (double)(dwi.z * fi + dwj.z * fj);
+                    ax -= fx;
+                    ay -= fy;
+                    az -= fz;
+                    de -= fx * (ex * vstar - vi.x) + fy * (ey * vstar - vi.y) + fz * (ez * vstar - vi.z);
+                    continue;
                 }
-                // f = dw_i m_j p* / rho_i^2 + dw_j m_j p* / rho_j^2 (src/gsph/g_fluid_force.cpp:158-165)
-                const T ps = (T)pstar;
-                const T fi = mj * ps * r2i;
-                const T fj = mj * ps * (T(1) / (rhoj * rhoj));
-                const double fx = (double)(dwi.x * fi + dwj.x * fj);
-                const double fy = (double)(dwi.y * fi + dwj.y * fj);
-                const double fz = (double)(dwi.z * fi + dwj.z * fj);
-                ax -= fx;
-                ay -= fy;
-                az -= fz;
-                de -= fx * (ex * vstar - vi.x) + fy * (ey * vstar - vi.y) + fz * (ez * vstar - vi.z);
-                continue;
             }
             const double4 sj = S.visc[j];
             const V3<T> dwij{(dwi.x + dwj.x) * T(0.5), (dwi.y + dwj.y) * T(0.5), (dwi.z + dwj.z) * T(0.5)};
@@ -396,12 +418,12 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
             const T vdwi = vij.x * dwi.x + vij.y * dwi.y + vij.z * dwi.z;
             const T vdwij = vij.x * dwij.x + vij.y * dwij.y + vij.z * dwij.z;
             T a_i, a_j, e_;
-            if(TYPE == SPHGPU_DISPH) {
+            if(TYPE == SPHGPU_DISPH || TYPE == SPHGPU_GDISPH) {
                 const T fij = T(1) - (T)si.z / (mj * uj);
                 const T fji = T(1) - (T)sj.z * mu_inv;
-                a_i = mj * (g2up * uj * fij + T(0.5) * pij);
-                a_j = mj * (g2u * (uj / Pj) * fji + T(0.5) * pij);
-                e_ = mj * g2up * uj * fij * vdwi + T(0.5) * mj * pij * vdwij + dac;
+                a_i = mj * (g2up * uj * fij * psi + T(0.5) * pij);
+                a_j = mj * (g2u * (uj / Pj) * fji * psj + T(0.5) * pij);
+                e_ = mj * g2up * uj * fij * psi * vdwi + T(0.5) * mj * pij * vdwij + dac;
             } else {
                 a_i = mj * (ppr * (T)si.z + T(0.5) * pij);
                 a_j = mj * (Pj / (rhoj * rhoj) * (T)sj.z + T(0.5) * pij);
@@ -453,6 +475,10 @@ void launch_force(sphgpu_ctx* c, MlpPairs mp, Harvest hv)
         k_force<T, GROUP, SPHGPU_GSPH, MODE><<<grid, FBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_plist,
                                                                            c->d_pcount, (int)c->pcap, c->d_dt,
                                                                            c->d_status, mp, hv);
+    } else if(type == SPHGPU_GDISPH) {
+        k_force<T, GROUP, SPHGPU_GDISPH, 0><<<grid, FBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_plist,
+                                                                          c->d_pcount, (int)c->pcap, c->d_dt,
+                                                                          c->d_status, mp, hv);
     } else {
         k_force<T, GROUP, SPHGPU_SSPH, 0><<<grid, FBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_plist, c->d_pcount,
                                                                         (int)c->pcap, c->d_dt, c->d_status, mp, hv);

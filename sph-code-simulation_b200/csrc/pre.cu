@@ -1,8 +1,11 @@
-// pre.cu — PreInteraction::calculation for ssph, disph and gsph.
+// pre.cu — PreInteraction::calculation for ssph, disph, gsph and gdisph.
 //
 // Reference: src/pre_interaction.cpp:39-283 (ssph, initial_smoothing,
 // newton_raphson), src/disph/d_pre_interaction.cpp:21-230 (disph),
-// src/gsph/g_pre_interaction.cpp:27-144 (gsph).
+// src/gsph/g_pre_interaction.cpp:27-144 (gsph), src/gdisph/gd_pre_interaction.cpp:
+// 29-280 (gdisph: the disph smoothing length, density and pressure, the gsph
+// MUSCL gradients, a mass-weighted Balsara switch normalised by density, and
+// without it the implicit alpha update weighted by mass x energy).
 //
 // A group of G lanes owns one particle and strides over its gather list
 // (ELL row, coalesced index loads; neighbour state as 32-byte double4 loads
@@ -55,7 +58,7 @@ __device__ __forceinline__ double r_within(const DevParams& P, double xi, double
 template <typename T, int TYPE>
 constexpr int pre_min_blocks()
 {
-    return (sizeof(T) == sizeof(float) && TYPE != SPHGPU_GSPH) ? 4 : 3;
+    return (sizeof(T) == sizeof(float) && TYPE != SPHGPU_GSPH && TYPE != SPHGPU_GDISPH) ? 4 : 3;
 }
 
 template <typename T, int G, int TYPE>
@@ -68,7 +71,11 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
     const long long warp = ((long long)blockIdx.x * PBLK + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * PBLK) >> 5;
     const double dt = *dtp;
-    const bool disph = TYPE == SPHGPU_DISPH, gsph = TYPE == SPHGPU_GSPH;
+    constexpr bool gdisph = TYPE == SPHGPU_GDISPH;
+    const bool disph = TYPE == SPHGPU_DISPH || gdisph, gsph = TYPE == SPHGPU_GSPH;
+    // AV switch sums weighted by m_j u_j and normalised by (gamma - 1) / P
+    // (disph; gdisph without the Balsara switch), else by m_j and 1 / rho
+    const bool av_energy = disph && !(gdisph && P.balsara);
     double hv_min = DBL_MAX;
     unsigned nonconv = 0;
 
@@ -133,7 +140,7 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
         double vsig = ti.w * 2.0;
         int nn = 0;
         const bool need_av = !gsph && (P.balsara || P.td_av);
-        const bool need_grad = gsph && P.gsph2;
+        const bool need_grad = (gsph || gdisph) && P.gsph2;
         for(int k = lane; k < cnt; k += G) {
             const int j = li[k];
             const double4 pj = S.pos[j];
@@ -169,12 +176,13 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
                 const T dwx = (T)dv.x * c, dwy = (T)dv.y * c, dwz = (T)dv.z * c;
                 const T vx = (T)(vi.x - vj.x), vy = (T)(vi.y - vj.y), vz = (T)(vi.z - vj.z);
                 if(need_av) {
-                    const T wgt = disph ? mj * (T)tj.z : mj;
+                    const T wgt = av_energy ? mj * (T)tj.z : mj;
                     divv -= wgt * (vx * dwx + vy * dwy + vz * dwz);
                     rx += (vy * dwz - vz * dwy) * wgt;
                     ry += (vz * dwx - vx * dwz) * wgt;
                     rz += (vx * dwy - vy * dwx) * wgt;
-                } else {
+                }
+                if(need_grad) {
                     const T du = mj * (T)(tj.z - ti.z);
                     gd[0] += dwx * mj;
                     gd[1] += dwy * mj;
@@ -248,7 +256,7 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
             // Balsara switch and time-dependent alpha (src/pre_interaction.cpp:115-161,
             // src/disph/d_pre_interaction.cpp:106-154)
             double dv_ = divS, r0 = rxS, r1 = ryS, r2 = rzS;
-            if(disph) {
+            if(av_energy) {
                 const double pinv = (gamma - 1.0) / pres_i;
                 dv_ *= pinv;
                 r0 *= pinv;
@@ -373,6 +381,9 @@ void launch_pre(sphgpu_ctx* c)
     } else if(type == SPHGPU_GSPH) {
         k_pre<T, GROUP, SPHGPU_GSPH><<<grid, PBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_glist, c->d_gcount,
                                                                    (int)c->gcap, c->d_dt, c->d_hvs, c->d_status);
+    } else if(type == SPHGPU_GDISPH) {
+        k_pre<T, GROUP, SPHGPU_GDISPH><<<grid, PBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_glist, c->d_gcount,
+                                                                     (int)c->gcap, c->d_dt, c->d_hvs, c->d_status);
     } else {
         k_pre<T, GROUP, SPHGPU_SSPH><<<grid, PBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_glist, c->d_gcount,
                                                                    (int)c->gcap, c->d_dt, c->d_hvs, c->d_status);

@@ -507,7 +507,7 @@ int tree_make(sphgpu_ctx* c)
     c->node_count = nnodes;
     // leaf order + permutation of the particle state
     k_leaf_order<<<grid_for(n, BLK), BLK, 0, st>>>(n, c->d_leaf_of_start, c->t.link, c->s.id, c->d_vals);
-    k_permute<<<grid_for(n, BLK), BLK, 0, st>>>(n, c->d_vals, c->s, c->alt, c->prm.sph_type == SPHGPU_GSPH,
+    k_permute<<<grid_for(n, BLK), BLK, 0, st>>>(n, c->d_vals, c->s, c->alt, c->prm.sph_type == SPHGPU_GSPH || c->prm.sph_type == SPHGPU_GDISPH,
                                                 c->d_inv);
     std::swap(c->s, c->alt);
     // mass and centre of mass

@@ -21,7 +21,8 @@ from conftest import golden, params_from_bytes, rel_err
 
 pytestmark = pytest.mark.gpu
 
-SMALL = ["evrard_ssph", "evrard_disph", "tube_gsph", "tube_gsph_hll", "shear_disph"]
+SMALL = ["evrard_ssph", "evrard_disph", "tube_gsph", "tube_gsph_hll", "shear_disph", "tube_gdisph",
+         "tube_gdisph_1st"]
 PRE_FIELDS = ["dens", "pres", "sml", "gradh", "balsara", "alpha"]
 
 
@@ -182,7 +183,7 @@ def test_pre_interaction_from_identical_state(gpu, O, name):
         if p.sph_type == gpu.GSPH and f in ("gradh", "balsara", "alpha"):
             continue
         _close(out[f], ref[f], f)
-    if p.sph_type == gpu.GSPH:
+    if p.sph_type in (gpu.GSPH, gpu.GDISPH) and p.gsph_2nd_order:
         for f in [x for x in gpu.FIELDS if x.startswith("grad_")]:
             sc = np.max(np.abs(ref[f])) + 1e-300
             _close(out[f], ref[f], f, scale=sc, median=1e-12, p999=1e-10)
