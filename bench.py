@@ -77,6 +77,8 @@ WORKLOADS = {
                           "tube_gsph", _tube, 2.0e6, 6.5e4),
     "tube_gsph_mlp": Workload("tube_gsph_mlp", "gsph shock tube 2.0M with the learned Riemann guess",
                               "tube_gsph", _tube, 2.0e6, 6.5e4, learned=True),
+    "tube_gdisph": Workload("tube_gdisph", "gdisph shock tube 2.0M (MUSCL + HLL, cubic, K=50, Balsara, TD-AV, AC)",
+                            "tube_gdisph", _tube, 2.0e6, 6.5e4),
     # The reference's algorithm (bit-exact oracle) turns non-finite near the
     # sphere's centre at t ~ 0.003-0.004 on this resolution whatever the CFL;
     # cflSound 0.05 / cflForce 0.025 keep 3 warm-up + 10 timed steps finite.

@@ -28,6 +28,8 @@ CASES = {
     "tube_gsph": lambda G: (G.config_params("tube_gsph", range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.1, 0.1)),
                             G.sample_shock_tube(0.01, ly=0.1)),
     "evrard_disph": lambda G: (G.config_params("evrard_disph"), G.sample_evrard(24)),
+    "tube_gdisph": lambda G: (G.config_params("tube_gdisph", range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.1, 0.1)),
+                              G.sample_shock_tube(0.01, ly=0.1)),
 }
 SPHERES = ("evrard_ssph", "evrard_disph")
 
