@@ -212,6 +212,43 @@ int sphgpu_integrate(sphgpu_ctx* ctx);
 int sphgpu_energies(sphgpu_ctx* ctx, double* kinetic, double* thermal,
                     double* potential, double* mom);
 
+/* ---- Snapshots in the reference's CSV v1 format ------------------------
+ * CSVWriter (src/writers/csv_writer.cpp:18-170) with the header of
+ * OutputManager::build_metadata (src/output_manager.cpp:254-299): code units,
+ * doubles as "%.*e" with `precision` digits (the reference's default 16),
+ * rows ordered by caller index with id = that index.  The reference's own
+ * plotting scripts and load_for_resume (src/output_manager.cpp:150-233) read
+ * these files. */
+typedef struct sphgpu_csv_meta {
+    int step;                      /* header "Step"                          */
+    double time;                   /* "Time (code)" and "Time (physical)"    */
+    int sph_type;                  /* enum sphgpu_sph_type; others: Unknown  */
+    int kernel;                    /* enum sphgpu_kernel; others: Unknown    */
+    double gamma, g_constant;
+    int neighbor_number;
+    int use_gravity, use_balsara, use_time_dependent_av;
+    double kinetic, thermal, potential;  /* "Total" is their sum          */
+    int precision;                 /* decimal digits after the point (1..30) */
+    const char* timestamp;         /* NULL or "": the current UTC time       */
+} sphgpu_csv_meta;
+/* The context's state (downloaded in caller order), its time, parameters
+   and device energies, written to `path`. */
+int sphgpu_write_csv(sphgpu_ctx* ctx, const char* path, int step, int precision);
+/* OutputManager::load_for_resume (src/output_manager.cpp:150-233) for a CSV
+   snapshot: its particles, in file order, become the context's state (as
+   sphgpu_upload) and its "Time (code)" the simulation time; *step (may be
+   NULL) receives its "Step". */
+int sphgpu_read_csv(sphgpu_ctx* ctx, const char* path, int* step);
+/* Host-only writer: n rows from host arrays indexed like sphgpu_download's
+   (NULL arrays print 0; ids NULL = 0..n-1).  Needs no device. */
+int sphgpu_csv_write_host(const char* path, int64_t n, const double* const* fields,
+                          const int64_t* ids, const sphgpu_csv_meta* meta);
+/* Reader (CSVWriter::read_metadata / read_particles, src/writers/csv_writer.cpp:
+   172-369): *n = the file's row count; with fields != NULL fills up to cap rows
+   (ERR_ARG when the file holds more); meta and ids may be NULL. */
+int sphgpu_csv_read_host(const char* path, int64_t* n, int64_t cap, double* const* fields,
+                         int64_t* ids, sphgpu_csv_meta* meta);
+
 /* Neighbour-walk implementation: 0 (default) = warp-level group walk with
    exact fallback for pairs on the search radius; 1 = per-lane walk that
    replays the reference's recursion test by test.  Both give the same sets;

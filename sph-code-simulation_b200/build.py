@@ -28,7 +28,7 @@ NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-rela
 EXACT = {"tree.cu", "walk.cu", "gravity.cu", "integrate.cu", "noalloc.cu"}
 SOURCES = ["scan_sort.cu", "tree.cu", "walk.cu", "pre.cu", "force.cu", "gravity.cu",
            "integrate.cu", "mlp.cu", "capi.cu", "noalloc.cu"]
-HOST_SOURCES = ["samples.cpp"]
+HOST_SOURCES = ["samples.cpp", "csv.cpp"]
 
 
 def _nvcc() -> str:
@@ -81,7 +81,7 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
     with ThreadPoolExecutor(max_workers=jobs) as ex:
         list(ex.map(run, cmds))
     if cmds or _newer(objs, LIB):
-        run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"])
+        run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lpthread"])
     return LIB
 
 

@@ -601,6 +601,63 @@ int sphgpu_integrate(sphgpu_ctx* c)
     return SPHGPU_OK;
 }
 
+int sphgpu_write_csv(sphgpu_ctx* c, const char* path, int step, int precision)
+{
+    SPHGPU_NEED_STATE(c);
+    if(!path) return fail(c, SPHGPU_ERR_ARG, "write_csv: no path");
+    if(precision < 1 || precision > 30) return fail(c, SPHGPU_ERR_ARG, "write_csv: precision must be 1..30");
+    static const int cols[20] = {SPHGPU_F_POS_X, SPHGPU_F_POS_Y, SPHGPU_F_POS_Z, SPHGPU_F_VEL_X, SPHGPU_F_VEL_Y,
+                                 SPHGPU_F_VEL_Z, SPHGPU_F_ACC_X, SPHGPU_F_ACC_Y, SPHGPU_F_ACC_Z, SPHGPU_F_MASS,
+                                 SPHGPU_F_DENS, SPHGPU_F_PRES, SPHGPU_F_ENE, SPHGPU_F_SML, SPHGPU_F_SOUND,
+                                 SPHGPU_F_ALPHA, SPHGPU_F_BALSARA, SPHGPU_F_GRADH, SPHGPU_F_PHI, SPHGPU_F_NEIGHBOR};
+    const int n = c->n;
+    std::vector<double> host((size_t)n * 20);
+    double* ptrs[SPHGPU_NFIELDS] = {};
+    for(int k = 0; k < 20; ++k) ptrs[cols[k]] = host.data() + (size_t)k * n;
+    int rc = sphgpu_download(c, ptrs);
+    if(rc < 0) return rc;
+    double e[6];
+    rc = energies(c, e);
+    if(rc < 0) return rc;
+    sphgpu_csv_meta m{};
+    m.step = step;
+    m.time = c->time;
+    m.sph_type = c->prm.sph_type;
+    m.kernel = c->prm.kernel;
+    m.gamma = c->prm.gamma;
+    m.g_constant = c->prm.g_constant;
+    m.neighbor_number = c->prm.neighbor_number;
+    m.use_gravity = c->prm.use_gravity;
+    m.use_balsara = c->prm.use_balsara_switch;
+    m.use_time_dependent_av = c->prm.use_time_dependent_av;
+    m.kinetic = e[0];
+    m.thermal = e[1];
+    m.potential = e[2];
+    m.precision = precision;
+    m.timestamp = nullptr;
+    rc = sphgpu_csv_write_host(path, n, ptrs, nullptr, &m);
+    if(rc < 0) return fail(c, SPHGPU_ERR_ARG, "write_csv: cannot write the file");
+    return SPHGPU_OK;
+}
+
+int sphgpu_read_csv(sphgpu_ctx* c, const char* path, int* step)
+{
+    if(!c || !path) return SPHGPU_ERR_ARG;
+    int64_t n = 0;
+    if(sphgpu_csv_read_host(path, &n, 0, nullptr, nullptr, nullptr) < 0 || n <= 0)
+        return fail(c, SPHGPU_ERR_ARG, "read_csv: not a CSV v1 snapshot with particles");
+    std::vector<double> host((size_t)n * SPHGPU_NFIELDS, 0.0);
+    double* ptrs[SPHGPU_NFIELDS] = {};
+    for(int k = 0; k < SPHGPU_NFIELDS; ++k) ptrs[k] = host.data() + (size_t)k * n;
+    sphgpu_csv_meta m{};
+    if(sphgpu_csv_read_host(path, &n, n, ptrs, nullptr, &m) < 0) return fail(c, SPHGPU_ERR_ARG, "read_csv: bad row");
+    const int rc = sphgpu_upload(c, n, ptrs);
+    if(rc < 0) return rc;
+    c->time = m.time;
+    if(step) *step = m.step;
+    return SPHGPU_OK;
+}
+
 int sphgpu_energies(sphgpu_ctx* c, double* K, double* U, double* W, double* mom)
 {
     SPHGPU_NEED_STATE(c);

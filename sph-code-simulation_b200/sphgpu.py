@@ -78,6 +78,48 @@ class Params(C.Structure):
         return out
 
 
+class CsvMeta(C.Structure):
+    """Header values of a CSV v1 snapshot (sphgpu_csv_meta)."""
+    _fields_ = [("step", C.c_int), ("time", C.c_double), ("sph_type", C.c_int), ("kernel", C.c_int),
+                ("gamma", C.c_double), ("g_constant", C.c_double), ("neighbor_number", C.c_int),
+                ("use_gravity", C.c_int), ("use_balsara", C.c_int), ("use_time_dependent_av", C.c_int),
+                ("kinetic", C.c_double), ("thermal", C.c_double), ("potential", C.c_double),
+                ("precision", C.c_int), ("timestamp", C.c_char_p)]
+
+
+CSV_FIELDS = ["pos_x", "pos_y", "pos_z", "vel_x", "vel_y", "vel_z", "acc_x", "acc_y", "acc_z", "mass", "dens",
+              "pres", "ene", "sml", "sound", "alpha", "balsara", "gradh", "phi", "neighbor"]
+
+
+def csv_write(path: str, fields: Dict[str, np.ndarray], meta: "CsvMeta", ids=None):
+    """Write host arrays as a CSV v1 snapshot (no device needed)."""
+    n = len(next(iter(fields.values()))) if fields else 0
+    ptrs, keep = _field_ptrs({k: v for k, v in fields.items() if k in FIELD_INDEX}, n, False)
+    idp = None
+    if ids is not None:
+        ids = np.ascontiguousarray(ids, dtype=np.int64)
+        idp = ids.ctypes.data_as(C.POINTER(C.c_int64))
+    rc = lib().sphgpu_csv_write_host(path.encode(), n, ptrs, idp, C.byref(meta))
+    if rc < 0:
+        raise SPHException(f"csv_write failed ({rc}) for {path}")
+
+
+def csv_read(path: str):
+    """(fields, ids, meta) of a CSV v1 snapshot."""
+    n = C.c_int64()
+    meta = CsvMeta()
+    if lib().sphgpu_csv_read_host(path.encode(), C.byref(n), 0, None, None, None) < 0:
+        raise SPHException(f"csv_read failed for {path}")
+    out = {f: np.zeros(n.value) for f in CSV_FIELDS}
+    ids = np.zeros(n.value, dtype=np.int64)
+    ptrs, _ = _field_ptrs(out, n.value, True)
+    rc = lib().sphgpu_csv_read_host(path.encode(), C.byref(n), n.value, ptrs,
+                                    ids.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(meta))
+    if rc < 0:
+        raise SPHException(f"csv_read failed ({rc}) for {path}")
+    return out, ids, meta
+
+
 class Counters(C.Structure):
     _fields_ = [(n, C.c_int64) for n in (
         "newton_nonconverged", "riemann_solves", "riemann_iterations", "riemann_fallbacks",
@@ -124,6 +166,10 @@ def lib() -> C.CDLL:
         "sphgpu_initialize": (C.c_int, [vp]),
         "sphgpu_integrate": (C.c_int, [vp]),
         "sphgpu_energies": (C.c_int, [vp, dp, dp, dp, dp]),
+        "sphgpu_write_csv": (C.c_int, [vp, C.c_char_p, C.c_int, C.c_int]),
+        "sphgpu_read_csv": (C.c_int, [vp, C.c_char_p, C.POINTER(C.c_int)]),
+        "sphgpu_csv_write_host": (C.c_int, [C.c_char_p, i64, dpp, i64p, C.POINTER(CsvMeta)]),
+        "sphgpu_csv_read_host": (C.c_int, [C.c_char_p, i64p, i64, dpp, i64p, C.POINTER(CsvMeta)]),
         "sphgpu_get_counters": (C.c_int, [vp, C.POINTER(Counters)]),
         "sphgpu_reset_counters": (C.c_int, [vp]),
         "sphgpu_enable_timing": (C.c_int, [vp, C.c_int]),
@@ -334,6 +380,20 @@ class Simulation:
         self._check(lib().sphgpu_energies(self._h, C.byref(k), C.byref(u), C.byref(w),
                                           C.cast(mom, C.POINTER(C.c_double))), "energies")
         return k.value, u.value, w.value, np.array(mom[:])
+
+    def write_csv(self, path: str, step: int = 0, precision: int = 16):
+        """Snapshot in the reference's CSV v1 format (caller order, code units)."""
+        self._check(lib().sphgpu_write_csv(self._h, path.encode(), int(step), int(precision)), "write_csv")
+
+    def read_csv(self, path: str) -> int:
+        """Resume from a CSV v1 snapshot (particles and time); returns its step."""
+        n = C.c_int64()
+        if lib().sphgpu_csv_read_host(path.encode(), C.byref(n), 0, None, None, None) < 0:
+            raise SPHException(f"read_csv: cannot read {path}")
+        step = C.c_int()
+        self._check(lib().sphgpu_read_csv(self._h, path.encode(), C.byref(step)), "read_csv")
+        self.n = n.value
+        return step.value
 
     def set_walk_mode(self, mode: int):
         """0 = group walk (default), 1 = per-lane walk (cross-check)."""

@@ -21,6 +21,11 @@ oracle/_ref/libsphref*.so, driven by oracle/ref_harness.cpp):
                      gdisph shock tube, first and second order): the
                      full particle state after Solver::initialize and after
                      each of two Solver::integrate steps, plus dt.
+  csv_snapshots.npz  Lines of two CSV v1 snapshots the reference ships
+                     (sample/sr_sod/results_coarse/snapshot_0000.csv: header
+                     and its first 64 particle rows; test/checkpoint_csv_resume/
+                     snapshot_0001.csv: header only), the byte-level check of
+                     the CSV writer.
   lists_<cfg>.npz    Distance-sorted neighbour lists (CSR) from
                      BHTree::neighbor_search and from exhaustive_search
                      (gather and is_ij) at the state after initialize.
@@ -160,6 +165,17 @@ def lists(name):
     print(f"lists_{name}: {len(out['tree_ij0_ids'])} gather / {len(out['tree_ij1_ids'])} pair entries")
 
 
+def csv_golden():
+    out = {}
+    for tag, rel, rows in (("sr_sod", "sample/sr_sod/results_coarse/snapshot_0000.csv", 64),
+                           ("resume", "test/checkpoint_csv_resume/snapshot_0001.csv", 0)):
+        with open(os.path.join(REFDIR, rel)) as f:
+            lines = f.read().split("\n")
+        out[tag] = np.array(lines[:51 + rows])
+    np.savez_compressed(os.path.join(OUT, "csv_snapshots.npz"), **out)
+    print("csv_snapshots:", {k: len(v) for k, v in out.items()})
+
+
 def main():
     O.build(reference=True)
     if not O.have_reference():
@@ -169,6 +185,7 @@ def main():
         small_steps(name)
     for name in ("evrard_ssph", "tube_gsph", "shear_disph"):
         lists(name)
+    csv_golden()
 
 
 if __name__ == "__main__":
