@@ -212,6 +212,26 @@ int sphgpu_integrate(sphgpu_ctx* ctx);
 int sphgpu_energies(sphgpu_ctx* ctx, double* kinetic, double* thermal,
                     double* potential, double* mom);
 
+/* ---- Lane-Emden relaxation ---------------------------------------------
+ * One step of Solver's relaxation loop (src/solver.cpp:779-829): tree, pre,
+ * force, gravity (when on); minus LaneEmdenRelaxation's analytic equilibrium
+ * acceleration (src/relaxation/lane_emden_relaxation.cpp:35-138) interpolated
+ * in the caller's table (LaneEmdenData, src/relaxation/lane_emden_data.cpp:
+ * 66-113; the reference reads it from data/lane_emden/n1.5_3d.dat); TimeStep's
+ * dt x 0.1 -> *dt_relax; v = 0, x += a dt^2 / 2.  `first` != 0 sets the sound
+ * speeds first, as the set-up before the loop does.  The simulation time is
+ * not advanced (the reference accumulates dt_relax separately). */
+typedef struct sphgpu_lane_emden {
+    double alpha_scaling;          /* r = alpha * xi                         */
+    double K;                      /* polytropic constant                    */
+    double xi_1;                   /* first zero of theta                    */
+    const double* xi;              /* npts ascending abscissae (host)        */
+    const double* theta;
+    const double* dtheta;          /* dtheta / dxi                           */
+    int64_t npts;
+} sphgpu_lane_emden;
+int sphgpu_relax_step(sphgpu_ctx* ctx, const sphgpu_lane_emden* le, int first, double* dt_relax);
+
 /* ---- Snapshots in the reference's CSV v1 format ------------------------
  * CSVWriter (src/writers/csv_writer.cpp:18-170) with the header of
  * OutputManager::build_metadata (src/output_manager.cpp:254-299): code units,

@@ -88,11 +88,13 @@ def _load(path: str, prefix: str) -> C.CDLL:
             getattr(L, f).argtypes = [C.c_int, C.c_double, C.c_double]
         L.oracle_riemann.restype = C.c_int
         L.oracle_riemann.argtypes = [C.c_int, dp, dp, C.c_double, dp, dp]
+        L.oracle_relax_step.argtypes = [vp, dp, dp, dp, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_int, dp]
     else:
         L.ref_create.restype = vp
         L.ref_create.argtypes = [C.c_void_p, C.c_int64, dpp]
         L.ref_energies.argtypes = [vp, dp, dp, dp]
         L.ref_module_times.argtypes = [vp, dp]
+        L.ref_relax_step.argtypes = [vp, C.c_char_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, dp]
     for name in ("destroy", "get", "set", "tree_make", "set_kernel", "pre", "force", "timestep", "predict",
                  "correct", "initialize", "integrate", "neighbor_lists", "get_dt", "set_dt", "get_time",
                  "get_h_per_v_sig", "last_error"):
@@ -215,6 +217,15 @@ class Oracle(_Base):
     def gravity_force(self, direct: bool = False):
         self._call("gravity", int(direct))
 
+    def relax_step(self, table, xi_1: float, alpha: float, K: float, first: bool) -> float:
+        """One Lane-Emden relaxation step; table = (xi, theta, dtheta) arrays.  Returns dt_relax."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in table]
+        dp = C.POINTER(C.c_double)
+        d = C.c_double()
+        self._call("relax_step", *[a.ctypes.data_as(dp) for a in arrs], len(arrs[0]), xi_1, alpha, K, int(first),
+                   C.byref(d))
+        return d.value
+
     def energies(self):
         k, u, w = C.c_double(), C.c_double(), C.c_double()
         mom = (C.c_double * 3)()
@@ -252,6 +263,12 @@ class Reference(_Base):
 
     def gravity_force(self, direct: bool = False):
         self._call("gravity")
+
+    def relax_step(self, refdir: str, alpha: float, rho_c: float, K: float, R: float, M: float) -> float:
+        """One step of the reference's relaxation loop.  Returns dt_relax."""
+        d = C.c_double()
+        self._call("relax_step", refdir.encode(), alpha, rho_c, K, R, M, C.byref(d))
+        return d.value
 
     def energies(self):
         k, u, w = C.c_double(), C.c_double(), C.c_double()

@@ -4,7 +4,7 @@
 // the reference's unmodified sources (src/bhtree.cpp, src/pre_interaction.cpp,
 // src/fluid_force.cpp, src/gravity_force.cpp, src/timestep.cpp,
 // src/simulation.cpp, src/exhaustive_search.cpp, src/disph/*.cpp,
-// src/gsph/*.cpp, src/gdisph/*.cpp) by oracle/Makefile into oracle/_ref/libsphref.so (tree
+// src/gsph/*.cpp, src/gdisph/*.cpp, src/relaxation/*.cpp) by oracle/Makefile into oracle/_ref/libsphref.so (tree
 // search) and oracle/_ref/libsphref_exh.so (-DEXHAUSTIVE_SEARCH).  It is the
 // checker the CPU restatement (oracle/sph_oracle.cpp) and the GPU path are
 // compared with, and the CPU baseline that bench.py --impl reference times.
@@ -38,6 +38,9 @@
 #include "gdisph/gd_fluid_force.hpp"
 #include "exhaustive_search.hpp"
 #include "exception.hpp"
+#include "relaxation/lane_emden_relaxation.hpp"
+
+#include <unistd.h>
 
 #include "sphgpu.h"
 
@@ -49,6 +52,7 @@ struct RefCtx {
     std::shared_ptr<SPHParameters> param;
     std::shared_ptr<Simulation> sim;
     std::shared_ptr<Module> timestep, pre, fforce, gforce;
+    std::shared_ptr<LaneEmdenRelaxation> relax;
     std::string err;
     double t_module[8] = {0};  // seconds: timestep, predict, tree, pre, force, gravity, correct, total
 };
@@ -367,6 +371,58 @@ int ref_integrate(void* h)
         correct(*c);
         t1 = now(); c->t_module[6] += t1 - t0;
         c->sim->update_time();
+    });
+}
+
+// One step of Solver's Lane-Emden relaxation loop (src/solver.cpp:779-829;
+// progress bar and snapshots left out).  The first call sets up
+// LaneEmdenRelaxation (it reads data/lane_emden/n1.5_3d.dat relative to the
+// working directory, so the call switches into `refdir` for that) and the
+// sound speeds, as src/solver.cpp:726-756 does before the loop.
+int ref_relax_step(void* h, const char* refdir, double alpha, double rho_c, double K, double R, double M,
+                   double* dt_relax)
+{
+    auto* c = static_cast<RefCtx*>(h);
+    return guarded(c, [&] {
+        auto& particles = c->sim->get_particles();
+        const int num = c->sim->get_particle_num();
+        if(!c->relax) {
+            c->relax = std::make_shared<LaneEmdenRelaxation>();
+            LaneEmdenRelaxationParams rp;
+            rp.alpha_scaling = alpha;
+            rp.rho_center = rho_c;
+            rp.K = K;
+            rp.R = R;
+            rp.M_total = M;
+            rp.G = c->param->gravity.constant;
+            rp.gamma = c->param->physics.gamma;
+            char cwd[4096];
+            if(!getcwd(cwd, sizeof(cwd)) || chdir(refdir) != 0) THROW_ERROR("cannot enter the reference tree");
+            c->relax->initialize(rp);
+            if(chdir(cwd) != 0) THROW_ERROR("cannot return to the working directory");
+            const real gamma = c->param->physics.gamma;
+            const real c_sound_factor = gamma * (gamma - 1.0);
+            for(int i = 0; i < num; ++i) particles[i].sound = std::sqrt(c_sound_factor * particles[i].ene);
+        }
+        c->sim->make_tree();
+        c->pre->calculation(c->sim);
+        c->fforce->calculation(c->sim);
+        if(c->param->gravity.is_valid) c->gforce->calculation(c->sim);
+        c->relax->apply_relaxation(c->sim, 0.0);
+        c->timestep->calculation(c->sim);
+        real dt = c->sim->get_dt();
+        dt *= 0.1;
+        auto* periodic = c->sim->get_periodic().get();
+        for(int i = 0; i < num; ++i) {
+            particles[i].vel[0] = 0.0;
+            particles[i].vel[1] = 0.0;
+            particles[i].vel[2] = 0.0;
+            particles[i].pos[0] += 0.5 * particles[i].acc[0] * dt * dt;
+            particles[i].pos[1] += 0.5 * particles[i].acc[1] * dt * dt;
+            particles[i].pos[2] += 0.5 * particles[i].acc[2] * dt * dt;
+            periodic->apply(particles[i].pos);
+        }
+        *dt_relax = dt;
     });
 }
 

@@ -1038,6 +1038,62 @@ struct Oracle {
         time += dt;
         return true;
     }
+
+    // LaneEmdenData::get_theta / dtheta_dxi (src/relaxation/lane_emden_data.cpp:66-113):
+    // linear interpolation in a table with ascending xi.
+    static real table_at(const real* x, const real* y, int64_t np, real xi)
+    {
+        const real* it = std::lower_bound(x, x + np, xi);
+        if(it == x + np) return 0.0;
+        if(it == x) return y[0];
+        const int64_t i1 = it - x, i0 = i1 - 1;
+        const real frac = (xi - x[i0]) / (x[i1] - x[i0]);
+        return y[i0] * (1.0 - frac) + y[i1] * frac;
+    }
+
+    // One step of the Lane-Emden relaxation loop (src/solver.cpp:779-829):
+    // SPH forces, minus LaneEmdenRelaxation::compute_relaxation_force
+    // (src/relaxation/lane_emden_relaxation.cpp:35-116), TimeStep dt x 0.1,
+    // v = 0 and x += a dt^2 / 2.  `first` sets the sound speeds as the set-up
+    // before the loop does (src/solver.cpp:744-752).
+    bool relax_step(const real* tx, const real* tth, const real* tdth, int64_t np, real xi1, real alpha, real K,
+                    bool first, real& dt_out)
+    {
+        if(first) {
+            const real cs = prm.gamma * (prm.gamma - 1.0);
+            for(int i = 0; i < s.n; ++i) s.f[SPHGPU_F_SOUND][i] = std::sqrt(cs * s.f[SPHGPU_F_ENE][i]);
+        }
+        if(!make_tree() || !pre_interaction() || !fluid_force() || !gravity(exhaustive)) return false;
+        const real gamma = prm.gamma;
+        for(int i = 0; i < s.n; ++i) {
+            const V3 p = s.pos(i);
+            const real r = norm(p);
+            if(r < 1e-12) continue;
+            const real xi = r / alpha;
+            if(xi >= xi1) continue;
+            const real theta = xi <= 0.0 ? 1.0 : table_at(tx, tth, np, xi);
+            const real dtheta = xi <= 0.0 ? 0.0 : table_at(tx, tdth, np, xi);
+            if(theta <= 0.0) continue;
+            const real prefactor = K * gamma * 1.5 / alpha;
+            const real a_r = -prefactor * std::pow(theta, gamma - 1.0) * dtheta;
+            const real rinv = 1.0 / r;
+            s.f[SPHGPU_F_ACC_X][i] -= -a_r * p.x * rinv;
+            s.f[SPHGPU_F_ACC_Y][i] -= -a_r * p.y * rinv;
+            s.f[SPHGPU_F_ACC_Z][i] -= -a_r * p.z * rinv;
+        }
+        timestep();
+        const real d = dt * 0.1;
+        for(int i = 0; i < s.n; ++i) {
+            for(int k = 0; k < 3; ++k) {
+                s.f[SPHGPU_F_VEL_X + k][i] = 0.0;
+                real& x = s.f[SPHGPU_F_POS_X + k][i];
+                x += 0.5 * s.f[SPHGPU_F_ACC_X + k][i] * d * d;
+                per.apply(x, k);
+            }
+        }
+        dt_out = d;
+        return true;
+    }
 };
 
 }  // namespace oracle
@@ -1128,6 +1184,13 @@ int oracle_correct(void* h)
 }
 int oracle_initialize(void* h) { return static_cast<Oracle*>(h)->initialize() ? 0 : -1; }
 int oracle_integrate(void* h) { return static_cast<Oracle*>(h)->integrate() ? 0 : -1; }
+
+int oracle_relax_step(void* h, const double* xi, const double* theta, const double* dtheta, int64_t np,
+                      double xi_1, double alpha, double K, int first, double* dt_relax)
+{
+    return static_cast<Oracle*>(h)->relax_step(xi, theta, dtheta, np, xi_1, alpha, K, first != 0, *dt_relax) ? 0
+                                                                                                             : -1;
+}
 
 void oracle_energies(void* h, double* K, double* U, double* W, double* mom)
 {

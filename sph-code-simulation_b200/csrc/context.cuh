@@ -53,6 +53,8 @@ struct sphgpu_ctx {
     double* d_dt = nullptr;          // Simulation::dt
     double* d_hvs = nullptr;         // Simulation::h_per_v_sig
     double* d_red = nullptr;         // reduction scratch
+    double* d_relax = nullptr;       // Lane-Emden table (xi, theta, dtheta) + dt_relax
+    int64_t relax_cap = 0;
     sphgpu::DevStatus* d_status = nullptr;
     sphgpu::DevStatus h_status{};
 

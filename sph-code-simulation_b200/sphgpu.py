@@ -78,6 +78,13 @@ class Params(C.Structure):
         return out
 
 
+class LaneEmden(C.Structure):
+    """A tabulated Lane-Emden solution and its scaling (sphgpu_lane_emden)."""
+    _fields_ = [("alpha_scaling", C.c_double), ("K", C.c_double), ("xi_1", C.c_double),
+                ("xi", C.POINTER(C.c_double)), ("theta", C.POINTER(C.c_double)),
+                ("dtheta", C.POINTER(C.c_double)), ("npts", C.c_int64)]
+
+
 class CsvMeta(C.Structure):
     """Header values of a CSV v1 snapshot (sphgpu_csv_meta)."""
     _fields_ = [("step", C.c_int), ("time", C.c_double), ("sph_type", C.c_int), ("kernel", C.c_int),
@@ -167,6 +174,7 @@ def lib() -> C.CDLL:
         "sphgpu_integrate": (C.c_int, [vp]),
         "sphgpu_energies": (C.c_int, [vp, dp, dp, dp, dp]),
         "sphgpu_write_csv": (C.c_int, [vp, C.c_char_p, C.c_int, C.c_int]),
+        "sphgpu_relax_step": (C.c_int, [vp, C.POINTER(LaneEmden), C.c_int, dp]),
         "sphgpu_read_csv": (C.c_int, [vp, C.c_char_p, C.POINTER(C.c_int)]),
         "sphgpu_csv_write_host": (C.c_int, [C.c_char_p, i64, dpp, i64p, C.POINTER(CsvMeta)]),
         "sphgpu_csv_read_host": (C.c_int, [C.c_char_p, i64p, i64, dpp, i64p, C.POINTER(CsvMeta)]),
@@ -380,6 +388,16 @@ class Simulation:
         self._check(lib().sphgpu_energies(self._h, C.byref(k), C.byref(u), C.byref(w),
                                           C.cast(mom, C.POINTER(C.c_double))), "energies")
         return k.value, u.value, w.value, np.array(mom[:])
+
+    def relax_step(self, xi, theta, dtheta, xi_1: float, alpha: float, K: float, first: bool = False) -> float:
+        """One Lane-Emden relaxation step; returns dt_relax."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (xi, theta, dtheta)]
+        dp = C.POINTER(C.c_double)
+        le = LaneEmden(alpha, K, xi_1, arrs[0].ctypes.data_as(dp), arrs[1].ctypes.data_as(dp),
+                       arrs[2].ctypes.data_as(dp), len(arrs[0]))
+        d = C.c_double()
+        self._check(lib().sphgpu_relax_step(self._h, C.byref(le), int(first), C.byref(d)), "relax_step")
+        return d.value
 
     def write_csv(self, path: str, step: int = 0, precision: int = 16):
         """Snapshot in the reference's CSV v1 format (caller order, code units)."""

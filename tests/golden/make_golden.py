@@ -26,6 +26,11 @@ oracle/_ref/libsphref*.so, driven by oracle/ref_harness.cpp):
                      and its first 64 particle rows; test/checkpoint_csv_resume/
                      snapshot_0001.csv: header only), the byte-level check of
                      the CSV writer.
+  relax_evrard.npz   Three steps of the reference's Lane-Emden relaxation loop
+                     on the ssph Evrard sample (N=12 lattice, alpha = 0.3,
+                     K = 0.5), with the reference's table
+                     data/lane_emden/n1.5_3d.dat (xi, theta, dtheta, xi_1):
+                     states after each step and dt_relax.
   lists_<cfg>.npz    Distance-sorted neighbour lists (CSR) from
                      BHTree::neighbor_search and from exhaustive_search
                      (gather and is_ij) at the state after initialize.
@@ -176,6 +181,36 @@ def csv_golden():
     print("csv_snapshots:", {k: len(v) for k, v in out.items()})
 
 
+RELAX_FIELDS = ["pos_x", "pos_y", "pos_z", "vel_x", "vel_y", "vel_z", "acc_x", "acc_y", "acc_z", "dens", "pres",
+                "sml", "sound", "phi"]
+
+
+def relax_golden(steps=3, alpha=0.3, K=0.5):
+    path = os.path.join(REFDIR, "data/lane_emden/n1.5_3d.dat")
+    tab = np.loadtxt(path, comments="#")
+    xi_1 = None
+    with open(path) as f:
+        for ln in f:
+            if ln.startswith("# xi_1"):
+                xi_1 = float(ln.split("=")[1])
+    p = G.config_params("evrard_ssph")
+    fields = G.sample_evrard(12)
+    ref = O.Reference(p, fields)
+    out = {"params": np.frombuffer(bytes(p), dtype=np.uint8), "xi": tab[:, 0], "theta": tab[:, 1],
+           "dtheta": tab[:, 2], "xi_1": xi_1, "alpha": alpha, "K": K}
+    for k in ("pos_x", "pos_y", "pos_z", "vel_x", "vel_y", "vel_z", "mass", "dens", "pres", "ene"):
+        out["ic_" + k] = fields[k]
+    dts = []
+    for s in range(steps):
+        dts.append(ref.relax_step(REFDIR, alpha, 1.0, K, 1.0, 1.0))
+        st = ref.download(RELAX_FIELDS)
+        for f, v in st.items():
+            out[f"s{s}_{f}"] = v
+    out["dt_relax"] = np.array(dts)
+    np.savez_compressed(os.path.join(OUT, "relax_evrard.npz"), **out)
+    print("relax_evrard: dt_relax", dts)
+
+
 def main():
     O.build(reference=True)
     if not O.have_reference():
@@ -186,6 +221,7 @@ def main():
     for name in ("evrard_ssph", "tube_gsph", "shear_disph"):
         lists(name)
     csv_golden()
+    relax_golden()
 
 
 if __name__ == "__main__":

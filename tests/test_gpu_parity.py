@@ -303,3 +303,25 @@ def test_gravity_bitexact_leaf_sizes(gpu, O, leaf):
             else:
                 scale = np.abs(ref[k]).max()
                 assert np.median(np.abs(out[k] - ref[k])) <= 1e-6 * scale, k
+
+
+def test_relaxation_against_reference_golden(gpu):
+    """Three Lane-Emden relaxation steps against the reference's own states
+    (the equilibrium term uses CUDA's pow, so agreement is to rounding)."""
+    g = golden("relax_evrard.npz")
+    p = params_from_bytes(gpu, g["params"])
+    fields = {k[3:]: g[k] for k in g.files if k.startswith("ic_")}
+    with gpu.Simulation(p) as sim:
+        sim.upload(fields)
+        for s in range(len(g["dt_relax"])):
+            d = sim.relax_step(g["xi"], g["theta"], g["dtheta"], float(g["xi_1"]), float(g["alpha"]), float(g["K"]),
+                               first=(s == 0))
+            assert d == pytest.approx(float(g["dt_relax"][s]), rel=1e-10)
+            out = sim.download()
+            for f in ("pos_x", "pos_y", "pos_z"):
+                _close(out[f], g[f"s{s}_{f}"], f"step {s} {f}", median=1e-14, p999=1e-12, worst=1e-10)
+            np.testing.assert_array_equal(out["vel_x"], 0.0)
+            amax = max(np.max(np.abs(g[f"s{s}_acc_{a}"])) for a in "xyz")
+            for a in "xyz":
+                _close(out[f"acc_{a}"], g[f"s{s}_acc_{a}"], f"step {s} acc_{a}", scale=amax, median=1e-12,
+                       p999=1e-9, worst=1e-7)

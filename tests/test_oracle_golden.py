@@ -116,3 +116,18 @@ def test_riemann_solvers(O):
     assert 0.25 < p < 0.35 and 0.8 < v < 1.0  # exact Sod star state p*=0.3031, u*=0.9274
     p, v, it = O.riemann(1, (0.0, -1.0, 1.0, 1.0), (0.0, 1.0, 1.0, 1.0), 1.4)
     assert (p, v, it) == (0.0, 0.0, 0)
+
+
+def test_oracle_relaxation_steps(G, O):
+    """Three Lane-Emden relaxation steps: bit-identical to the reference's."""
+    g = golden("relax_evrard.npz")
+    p = params_from_bytes(G, g["params"])
+    fields = {k[3:]: g[k] for k in g.files if k.startswith("ic_")}
+    o = O.Oracle(p, fields)
+    table = (g["xi"], g["theta"], g["dtheta"])
+    for s in range(len(g["dt_relax"])):
+        d = o.relax_step(table, float(g["xi_1"]), float(g["alpha"]), float(g["K"]), s == 0)
+        assert d == g["dt_relax"][s]
+        st = o.download()
+        for f in ("pos_x", "pos_y", "pos_z", "vel_x", "acc_x", "acc_y", "acc_z", "dens", "sml", "sound", "phi"):
+            np.testing.assert_array_equal(st[f], g[f"s{s}_{f}"], err_msg=f"step {s} {f}")
