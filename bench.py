@@ -348,7 +348,38 @@ def run_gpu(args, rank: int, world: int, local: int):
     }
 
 
+def _gpu_local_cpus(local: int):
+    """CPUs on the GPU's own NUMA node (sysfs local_cpulist of its PCI device), or None."""
+    try:
+        import pynvml
+        pynvml.nvmlInit()
+        bus = pynvml.nvmlDeviceGetPciInfo(pynvml.nvmlDeviceGetHandleByIndex(local)).busId
+        bus = (bus.decode() if isinstance(bus, bytes) else bus).lower()
+        dom, rest = bus.split(":", 1)
+        path = f"/sys/bus/pci/devices/{int(dom, 16):04x}:{rest}/local_cpulist"
+        cpus = set()
+        for part in open(path).read().strip().split(","):
+            a, _, b = part.partition("-")
+            cpus.update(range(int(a), int(b or a) + 1))
+        return cpus & os.sched_getaffinity(0) or None
+    except Exception:
+        return None
+
+
 def run_e2e(args, G, fields, world, wl):
+    # pinned buffers and the copy loop on the GPU's own NUMA node (first-touch
+    # placement of the host pages); the previous affinity is restored after
+    saved = os.sched_getaffinity(0)
+    local_cpus = _gpu_local_cpus(int(os.environ.get("LOCAL_RANK", "0")))
+    if local_cpus:
+        os.sched_setaffinity(0, local_cpus)
+    try:
+        return _run_e2e(args, G, fields, world, wl)
+    finally:
+        os.sched_setaffinity(0, saved)
+
+
+def _run_e2e(args, G, fields, world, wl):
     import ctypes
     n = len(fields["pos_x"])
     p = wl.params(G, G.FP64)
@@ -370,17 +401,27 @@ def run_e2e(args, G, fields, world, wl):
         ptr_out[G.FIELD_INDEX[f]] = ctypes.cast(t.data_ptr(), ctypes.POINTER(ctypes.c_double))
     L = G.lib()
 
+    phase = [0.0, 0.0, 0.0]   # host seconds: upload, integrate, download
+
     def step():
+        t0 = time.perf_counter()
         rc = L.sphgpu_upload(sim._h, n, ptr_in)
         assert rc >= 0, sim._err()
+        t1 = time.perf_counter()
         L.sphgpu_set_initial_smoothing(sim._h, 0)
         rc = L.sphgpu_integrate(sim._h)
         assert rc >= 0, sim._err()
+        t2 = time.perf_counter()
         rc = L.sphgpu_download(sim._h, ptr_out)
         assert rc >= 0, sim._err()
+        t3 = time.perf_counter()
+        phase[0] += t1 - t0
+        phase[1] += t2 - t1
+        phase[2] += t3 - t2
 
     for _ in range(max(1, args.warmup)):
         step()
+    phase[:] = [0.0, 0.0, 0.0]
     barrier()
     L.sphgpu_timer_start(sim._h)
     for _ in range(args.steps):
@@ -389,10 +430,25 @@ def run_e2e(args, G, fields, world, wl):
     L.sphgpu_timer_stop(sim._h, ctypes.byref(ms))
     barrier()
     ms_max = max_over_ranks(ms.value)
+    # the same copies without the step: what the host link gives on this box
+    reps = 3
+    L.sphgpu_timer_start(sim._h)
+    for _ in range(reps):
+        rc = L.sphgpu_upload(sim._h, n, ptr_in)
+        assert rc >= 0, sim._err()
+        rc = L.sphgpu_download(sim._h, ptr_out)
+        assert rc >= 0, sim._err()
+    cms = ctypes.c_double()
+    L.sphgpu_timer_stop(sim._h, ctypes.byref(cms))
     sim.close()
+    h2d, d2h = n * 8 * len(E2E_IN), n * 8 * len(E2E_OUT)
+    copy_ms = cms.value / reps
     return {"value": whole_job_value(n * args.steps, world, ms_max), "unit": UNIT,
-            "h2d_bytes_per_step": n * 8 * len(E2E_IN), "d2h_bytes_per_step": n * 8 * len(E2E_OUT),
-            "ms_per_step": ms_max / args.steps}
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "ms_per_step": ms_max / args.steps, "copy_ms_per_step": copy_ms,
+            "copy_gbs": (h2d + d2h) / (copy_ms * 1e-3) / 1e9 if copy_ms > 0 else None,
+            "host_ms_per_step": {k: round(1e3 * v / max(args.steps, 1), 3)
+                                 for k, v in zip(("upload", "integrate", "download"), phase)}}
 
 
 class _QuietStdout:

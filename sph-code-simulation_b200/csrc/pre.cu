@@ -100,8 +100,13 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
                 const double hb = h;
                 T d = 0, dd = 0;
                 const KernH<T> kh(P.kernel, (T)h);
+                // the next candidate's index is fetched one iteration ahead,
+                // so the position load does not wait on the list load
+                int jn = lane < cnt ? __ldg(&li[lane]) : 0;
                 for(int k = lane; k < cnt; k += G) {
-                    const double4 pj = S.pos[li[k]];
+                    const int jc = jn;
+                    if(k + G < cnt) jn = __ldg(&li[k + G]);
+                    const double4 pj = S.pos[jc];
                     Vec3d dv;
                     const double r = r_within(P, pi.x, pi.y, pi.z, pj, h, dv);
                     if(r >= 0.0 && r < h) {
@@ -141,8 +146,10 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
         int nn = 0;
         const bool need_av = !gsph && (P.balsara || P.td_av);
         const bool need_grad = (gsph || gdisph) && P.gsph2;
+        int jn2 = lane < cnt ? __ldg(&li[lane]) : 0;
         for(int k = lane; k < cnt; k += G) {
-            const int j = li[k];
+            const int j = jn2;
+            if(k + G < cnt) jn2 = __ldg(&li[k + G]);
             const double4 pj = S.pos[j];
             Vec3d dv;
             const double r = r_within(P, pi.x, pi.y, pi.z, pj, h, dv);
