@@ -164,6 +164,24 @@ public:
         return v;
     }
     void make_tree() { check(sphgpu_tree_make(m_ctx)); }
+    // OutputManager::write_snapshot / load_for_resume in the CSV v1 format
+    void write_csv(const std::string& path, int step, int precision = 16)
+    {
+        check(sphgpu_write_csv(m_ctx, path.c_str(), step, precision));
+    }
+    int read_csv(const std::string& path)
+    {
+        int step = 0;
+        check(sphgpu_read_csv(m_ctx, path.c_str(), &step));
+        return step;
+    }
+    // one step of Solver's Lane-Emden relaxation loop; returns dt_relax
+    double relax_step(const sphgpu_lane_emden& le, bool first)
+    {
+        double d = 0.0;
+        check(sphgpu_relax_step(m_ctx, &le, first ? 1 : 0, &d));
+        return d;
+    }
     std::shared_ptr<BHTree> get_tree();
 };
 
