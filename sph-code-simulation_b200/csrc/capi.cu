@@ -383,9 +383,7 @@ int sphgpu_destroy(sphgpu_ctx* c)
     if(c->d_mlp) cudaFree(c->d_mlp);
     if(c->d_mlp_master) cudaFree(c->d_mlp_master);
     if(c->d_relax) cudaFree(c->d_relax);
-    if(c->d_mlp_feat) cudaFree(c->d_mlp_feat);
-    if(c->d_mlp_y) cudaFree(c->d_mlp_y);
-    if(c->d_mlp_rows) cudaFree(c->d_mlp_rows);
+    if(c->d_mlp_defer) cudaFree(c->d_mlp_defer);
     if(c->d_harvest) cudaFree(c->d_harvest);
     if(c->d_harvest_count) cudaFree(c->d_harvest_count);
     stage_flush(c);

@@ -61,10 +61,11 @@ struct sphgpu_ctx {
     // learned Riemann guess (BF16 weights + FP32 biases on device)
     void* d_mlp = nullptr;            // BF16 / FP32 image read by the kernels
     float* d_mlp_master = nullptr;    // FP32 master parameters + Adam moments
-    uint4* d_mlp_feat = nullptr;      // per pair slot: scaled features (bf16)
-    float* d_mlp_y = nullptr;         // per pair slot: network output
-    unsigned long long* d_mlp_rows = nullptr;  // compacted feature rows of the current call
-    int64_t mlp_slots = 0;
+    // deferred pairs of the learned path: rows (features, pair keys, network
+    // output, sort buffers) and per-particle row ranges, in one allocation
+    void* d_mlp_defer = nullptr;
+    int64_t mlp_rcap = 0;             // rows the allocation holds
+    int64_t mlp_ncap = 0;             // particles the allocation holds
     bool have_mlp = false;
     std::vector<float> mlp_master;
     // pair-state harvesting (training data from the plain solver's own runs)

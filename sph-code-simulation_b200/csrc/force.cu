@@ -20,6 +20,7 @@
 
 #include "context.cuh"
 #include "mlp.cuh"
+#include "scan_sort.cuh"
 
 namespace sphgpu {
 
@@ -93,8 +94,8 @@ __device__ __forceinline__ double vl_ustar(double p, double ul, double pl, doubl
 
 // Screen of the learned start: one Newton step from the reference's
 // linearised guess (src/gsph/g_fluid_force.cpp:244-246).  Returns the relative
-// change and the stepped pressure.  Not inlined, so the feature pass and the
-// force pass take the same decision for the same pair.
+// change and the stepped pressure.  Kept out of line: the pair loops that call
+// it are register-bound.
 __device__ __noinline__ double learned_screen(double ul, double pl, double vl, double cl, double ur, double pr,
                                               double vr, double cr, double g1, double g2, double& q1)
 {
@@ -104,13 +105,13 @@ __device__ __noinline__ double learned_screen(double ul, double pl, double vl, d
     return fabs(q1 - q0) / q1;
 }
 
-__device__ __forceinline__ bool learned_needed(const double* L, const double* R, double gamma)
+// The screen for states with positive densities and pressures: relative change
+// `ch` and stepped pressure `q1`; the network's guess is needed when ch >= 1e-2.
+__device__ __forceinline__ void pair_screen(const double* L, const double* R, double gamma, double& ch, double& q1)
 {
-    if(!(L[1] > 0.0 && R[1] > 0.0 && L[2] > 0.0 && R[2] > 0.0)) return false;
     const double g2 = 1.0 + gamma, g1 = 0.5 * g2 / gamma;
     const double cl = sqrt(gamma * L[2] * L[1]), cr = sqrt(gamma * R[2] * R[1]);
-    double q1;
-    return !(learned_screen(L[0], L[2], 1.0 / L[1], cl, R[0], R[2], 1.0 / R[1], cr, g1, g2, q1) < 1e-2);
+    ch = learned_screen(L[0], L[2], 1.0 / L[1], cl, R[0], R[2], 1.0 / R[1], cr, g1, g2, q1);
 }
 
 // Iterative solver (src/gsph/g_fluid_force.cpp:209-304).  Plain form: FP64
@@ -119,9 +120,11 @@ __device__ __forceinline__ bool learned_needed(const double* L, const double* R,
 // (below; y = the network's log(p_star / p_L), read only when the screen
 // rejects the linearised start), runs at most `budget` iterations to a 1e-10
 // relative change (in FP64) and falls back to the plain start on failure.
+// A screen the caller already ran is passed as (scr_ch >= 0, scr_q1).
 template <typename T>
 __device__ void riemann_iterative(const double* L, const double* R, double gamma, bool learned, float y, int budget,
-                                  double& pstar, double& vstar, int& iters, int& fallback)
+                                  double& pstar, double& vstar, int& iters, int& fallback, double scr_ch = -1.0,
+                                  double scr_q1 = 0.0)
 {
     const double ul = L[0], rhol = L[1], pl = L[2];
     const double ur = R[0], rhor = R[1], pr = R[2];
@@ -146,8 +149,8 @@ __device__ void riemann_iterative(const double* L, const double* R, double gamma
         // otherwise Newton restarts from the network's guess.  Either way
         // Newton runs to a 1e-10 relative change within `budget` iterations,
         // else the reference's solver takes over.
-        double q1;
-        const double ch = learned_screen(ul, pl, vl, cl, ur, pr, vr, cr, g1, g2, q1);
+        double q1 = scr_q1;
+        const double ch = scr_ch >= 0.0 ? scr_ch : learned_screen(ul, pl, vl, cl, ur, pr, vr, cr, g1, g2, q1);
         iters = 1;
         const double guess = pl * exp((double)y);
         p = (ch < 1e-2 || !(guess > 0.0 && guess < 1e300)) ? q1 : guess;
@@ -195,8 +198,10 @@ __device__ void riemann_iterative(const double* L, const double* R, double gamma
     vstar = vl_ustar(p, ul, pl, cl, ur, pr, cr, g1);
 }
 
-// MODE: 0 = force (optionally harvesting pair states), 1 = GSPH features of
-// the learned guess only (no force written), 2 = force with the learned guess.
+// MODE: 0 = force (optionally harvesting pair states); 3 = force with the
+// learned guess, deferring the pairs whose linearised start the screen
+// rejects (their features and pair slots go to the MlpPairs rows); 4 = the
+// deferred pairs only, with the network's guess, added to acc.
 // Minimum resident blocks per SM (caps registers; measured on B200).
 template <typename T, int TYPE>
 constexpr int force_min_blocks()
@@ -220,7 +225,8 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
     for(long long wb = warp * GPW; wb < n; wb += nwarps * GPW) {
         const int i = (int)(wb + ((threadIdx.x & 31) / G));
         const bool valid = i < n;
-        const int cnt = valid ? min(count[i], cap) : 0;
+        const int cnt = valid ? (MODE == 4 ? mp.dcount[i] : min(count[i], cap)) : 0;
+        if(MODE == 4 && !__any_sync(FULL_MASK, cnt > 0)) continue;
         const int* li = list + (size_t)(valid ? i : 0) * (size_t)cap;
         const double4 pi = valid ? S.pos[i] : make_double4(0, 0, 0, 0);
         const double4 vi = valid ? S.vel[i] : make_double4(0, 0, 0, 1);
@@ -245,7 +251,14 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
         const T r2i = T(1) / (rhoi * rhoi);
         double ax = 0, ay = 0, az = 0, de = 0;
         for(int k = lane; k < cnt; k += G) {
-            const int j = li[k];
+            float yq = 0.f;
+            int kk = k;
+            if(MODE == 4) {
+                const int row = mp.dstart[i] + k;
+                kk = (int)(mp.skeys[row] - (uint64_t)i * (uint64_t)cap);
+                yq = mp.y[mp.svals[row]];
+            }
+            const int j = li[kk];
             const double4 pj = S.pos[j];
             const Vec3d d = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
             const double r = sqrt(abs2x(d));
@@ -329,25 +342,33 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
                     psj = (T)pg / Pj;
                 }
                 if constexpr(TYPE == SPHGPU_GSPH) {
-                    if(MODE == 1) {
-                        // features only for the pairs whose linearised start the
-                        // screen rejects, compacted, with the pair slot alongside
-                        if(learned_needed(Lst, Rst, gamma)) {
+                    const bool states_ok = Lst[1] > 0.0 && Rst[1] > 0.0 && Lst[2] > 0.0 && Rst[2] > 0.0;
+                    double scr_ch = -1.0, scr_q1 = 0.0;
+                    if(MODE == 3 && states_ok) pair_screen(Lst, Rst, gamma, scr_ch, scr_q1);
+                    if(MODE == 3 && !(scr_ch < 1e-2) && states_ok) {
+                        // deferred to the completion pass, which solves it from
+                        // the network's guess; with the row list full the pair
+                        // is solved here from the linearised start instead
+                        const unsigned long long row = atomicAdd(mp.rows, 1ull);
+                        if((long long)row < mp.rcap) {
                             float x[MLP_IN];
                             mlp_features(Lst, Rst, gamma, x);
-                            const unsigned long long row = atomicAdd(mp.rows, 1ull);
-                            atomicAdd(&st->mlp_guesses, 1ull);
                             mp.feat[row] = make_uint4(pack_bf16x2(x[0], x[1]), pack_bf16x2(x[2], x[3]),
-                                                      pack_bf16x2(x[4], 0.f), (unsigned)((size_t)i * cap + k));
+                                                      pack_bf16x2(x[4], 0.f), 0u);
+                            mp.keys[row] = (uint64_t)i * (uint64_t)cap + (uint64_t)k;
+                            atomicAdd(&st->mlp_guesses, 1ull);
+                            continue;
                         }
-                        continue;
                     }
                     double pstar, vstar;
                     if(P.riemann == SPHGPU_RIEMANN_ITERATIVE) {
                         int it = 0, fb = 0;
-                        const bool learned = MODE == 2 && Lst[1] > 0.0 && Rst[1] > 0.0 && Lst[2] > 0.0 && Rst[2] > 0.0;
-                        riemann_iterative<T>(Lst, Rst, gamma, learned, learned ? mp.y[(size_t)i * cap + k] : 0.f,
-                                             P.mlp_max_newton, pstar, vstar, it, fb);
+                        // learned start: the linearised guess where the screen
+                        // accepts it, else the network's (a NaN guess selects
+                        // the linearised one)
+                        const bool learned = (MODE == 3 || MODE == 4) && states_ok;
+                        riemann_iterative<T>(Lst, Rst, gamma, learned, MODE == 4 ? yq : __int_as_float(0x7fc00000),
+                                             P.mlp_max_newton, pstar, vstar, it, fb, scr_ch, scr_q1);
                         ++solves;
                         iters += it;
                         fallbacks += fb;
@@ -438,9 +459,16 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
         ay = group_sum<G>(ay);
         az = group_sum<G>(az);
         de = group_sum<G>(de);
-        if(MODE != 1 && valid && lane == 0) S.acc[i] = make_double4(ax, ay, az, de);
+        if(MODE == 4) {
+            if(cnt > 0 && lane == 0) {
+                const double4 a0 = S.acc[i];
+                S.acc[i] = make_double4(a0.x + ax, a0.y + ay, a0.z + az, a0.w + de);
+            }
+        } else if(valid && lane == 0) {
+            S.acc[i] = make_double4(ax, ay, az, de);
+        }
     }
-    if(TYPE == SPHGPU_GSPH && MODE != 1) {
+    if(TYPE == SPHGPU_GSPH) {
         for(int o = 16; o > 0; o >>= 1) {
             solves += __shfl_xor_sync(FULL_MASK, solves, o);
             iters += __shfl_xor_sync(FULL_MASK, iters, o);
@@ -526,6 +554,60 @@ __global__ void k_riemann_batch(const double* __restrict__ st, long long n, int 
     if(fb) fb[r] = f;
 }
 
+// One allocation for the deferred rows of the learned path (256-byte aligned
+// pieces); with base == nullptr only the total size is computed.
+struct DeferLayout {
+    uint4* feat;
+    uint64_t *keys, *keys_alt;
+    float* y;
+    uint32_t *vals, *vals_alt;
+    void* scratch;
+    int *dstart, *dcount;
+    unsigned long long* rows;
+    size_t total;
+};
+
+DeferLayout defer_layout(int64_t rcap, int64_t n, void* base)
+{
+    DeferLayout L{};
+    char* b = static_cast<char*>(base);
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        void* p = b ? b + off : nullptr;
+        off += (bytes + 255) & ~(size_t)255;
+        return p;
+    };
+    L.feat = static_cast<uint4*>(take(sizeof(uint4) * (size_t)rcap));
+    L.keys = static_cast<uint64_t*>(take(sizeof(uint64_t) * (size_t)rcap));
+    L.keys_alt = static_cast<uint64_t*>(take(sizeof(uint64_t) * (size_t)rcap));
+    L.y = static_cast<float*>(take(sizeof(float) * (size_t)rcap));
+    L.vals = static_cast<uint32_t*>(take(sizeof(uint32_t) * (size_t)rcap));
+    L.vals_alt = static_cast<uint32_t*>(take(sizeof(uint32_t) * (size_t)rcap));
+    L.scratch = take(radix_scratch_bytes((int)rcap));
+    L.dstart = static_cast<int*>(take(sizeof(int) * (size_t)n));
+    L.dcount = static_cast<int*>(take(sizeof(int) * (size_t)n));
+    L.rows = static_cast<unsigned long long*>(take(sizeof(unsigned long long)));
+    L.total = off;
+    return L;
+}
+
+__global__ void k_iota(uint32_t* v, int n)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if(r < n) v[r] = (uint32_t)r;
+}
+
+// Per particle, the first sorted row and the number of rows of its deferred pairs.
+__global__ void k_defer_ranges(const uint64_t* __restrict__ skeys, int n, uint64_t cap, int* __restrict__ dstart,
+                               int* __restrict__ dcount)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if(r >= n) return;
+    const uint64_t p = skeys[r] / cap;
+    if(r == 0 || skeys[r - 1] / cap != p) dstart[p] = r;
+    atomicAdd(&dcount[p], 1);
+}
+
 }  // namespace
 
 int fluid_force(sphgpu_ctx* c)
@@ -538,32 +620,59 @@ int fluid_force(sphgpu_ctx* c)
     if(rc_walk < 0) return rc_walk;
     stage_begin(c, SPHGPU_T_FORCE);
     Harvest hv{c->d_harvest, c->d_harvest_count, c->harvest_cap, c->harvest_mod, 0u};
-    MlpPairs mp{nullptr, nullptr, nullptr};
+    MlpPairs mp{};
     int launches = 1;
     if(learned) {
         const int64_t slots = (int64_t)c->n * c->pcap;
         if(slots > 0xFFFFFFFFLL) return fail(c, SPHGPU_ERR_ARG, "learned guess: more than 2^32 pair slots");
-        if(slots > c->mlp_slots) {
-            if(c->d_mlp_feat) cudaFree(c->d_mlp_feat);
-            if(c->d_mlp_y) cudaFree(c->d_mlp_y);
-            c->d_mlp_feat = nullptr;
-            c->d_mlp_y = nullptr;
-            SPHGPU_CUDA(c, cudaMalloc(&c->d_mlp_feat, sizeof(uint4) * (size_t)slots));
-            SPHGPU_CUDA(c, cudaMalloc(&c->d_mlp_y, sizeof(float) * (size_t)slots));
-            c->mlp_slots = slots;
+        // room for 1/16 of all pair slots (the screen rejects well under 1%)
+        const int64_t rcap = std::max<int64_t>(1 << 20, slots / 16);
+        if(rcap > c->mlp_rcap || c->n > c->mlp_ncap) {
+            if(c->d_mlp_defer) cudaFree(c->d_mlp_defer);
+            c->d_mlp_defer = nullptr;
+            c->mlp_rcap = 0;
+            const size_t bytes = defer_layout(rcap, c->n, nullptr).total;
+            SPHGPU_CUDA(c, cudaMalloc(&c->d_mlp_defer, bytes));
+            c->mlp_rcap = rcap;
+            c->mlp_ncap = c->n;
         }
-        if(!c->d_mlp_rows) SPHGPU_CUDA(c, cudaMalloc(&c->d_mlp_rows, sizeof(unsigned long long)));
-        SPHGPU_CUDA(c, cudaMemsetAsync(c->d_mlp_rows, 0, sizeof(unsigned long long), c->stream));
-        mp.feat = c->d_mlp_feat;
-        mp.y = c->d_mlp_y;
-        mp.rows = c->d_mlp_rows;
-        if(c->prm.precision == SPHGPU_MIXED) launch_force<float, 1>(c, mp, hv);
-        else launch_force<double, 1>(c, mp, hv);
-        const int rc = mlp_infer_pairs(c, c->d_mlp_rows, slots);
-        if(rc < 0) return rc;
-        if(c->prm.precision == SPHGPU_MIXED) launch_force<float, 2>(c, mp, hv);
-        else launch_force<double, 2>(c, mp, hv);
-        launches = 3;
+        DeferLayout L = defer_layout(c->mlp_rcap, c->mlp_ncap, c->d_mlp_defer);
+        SPHGPU_CUDA(c, cudaMemsetAsync(L.rows, 0, sizeof(unsigned long long), c->stream));
+        mp.feat = L.feat;
+        mp.keys = L.keys;
+        mp.rows = L.rows;
+        mp.rcap = c->mlp_rcap;
+        // pass 1: every pair the screen accepts; the others become rows
+        if(c->prm.precision == SPHGPU_MIXED) launch_force<float, 3>(c, mp, hv);
+        else launch_force<double, 3>(c, mp, hv);
+        SPHGPU_LAUNCH_CHECK(c, "FluidForce");
+        unsigned long long rows = 0;
+        SPHGPU_CUDA(c, cudaMemcpyAsync(&rows, L.rows, sizeof(rows), cudaMemcpyDeviceToHost, c->stream));
+        SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+        rows = std::min<unsigned long long>(rows, (unsigned long long)c->mlp_rcap);
+        if(rows > 0) {
+            const int nr = (int)rows;
+            const int rc = mlp_infer_rows(c, L.feat, L.y, nr);
+            if(rc < 0) return rc;
+            // rows sorted by pair key: each particle's deferred pairs in slot order
+            k_iota<<<grid_for(nr, 256), 256, 0, c->stream>>>(L.vals, nr);
+            int bits = 1;
+            while(bits < 32 && (1ull << bits) < (unsigned long long)slots) ++bits;
+            uint64_t *kk = L.keys, *ka = L.keys_alt;
+            uint32_t *vv = L.vals, *va = L.vals_alt;
+            launches += 2 + radix_sort(kk, vv, ka, va, nr, (bits + 7) / 8 * 8, L.scratch, c->stream);
+            SPHGPU_CUDA(c, cudaMemsetAsync(L.dcount, 0, sizeof(int) * (size_t)c->n, c->stream));
+            k_defer_ranges<<<grid_for(nr, 256), 256, 0, c->stream>>>(kk, nr, (uint64_t)c->pcap, L.dstart, L.dcount);
+            mp.y = L.y;
+            mp.skeys = kk;
+            mp.svals = vv;
+            mp.dstart = L.dstart;
+            mp.dcount = L.dcount;
+            // pass 2: the deferred pairs from the network's guess, added to acc
+            if(c->prm.precision == SPHGPU_MIXED) launch_force<float, 4>(c, mp, hv);
+            else launch_force<double, 4>(c, mp, hv);
+            launches += 2;
+        }
     } else {
         if(c->prm.precision == SPHGPU_MIXED) launch_force<float, 0>(c, mp, hv);
         else launch_force<double, 0>(c, mp, hv);

@@ -191,17 +191,13 @@ __device__ __forceinline__ void load_input(const uint4* __restrict__ feat, long 
 
 constexpr int IBLK = 128;
 
-// y for feature rows: y[row], or with `scatter` y[feat[row].w] (compacted
-// pair rows carrying their slot).  With d_rows != null the row count is read
-// on the device (at most `rows`).
+// y[row] for feature rows (8 bf16 per row, 5 used).
 __global__ void __launch_bounds__(IBLK) k_mlp_infer(MlpDev m, const uint4* __restrict__ feat, float* __restrict__ y,
-                                                    long long rows, const unsigned long long* __restrict__ d_rows,
-                                                    bool scatter)
+                                                    long long rows)
 {
     __shared__ SmemNet s;
     load_net(s, m);
     __syncthreads();
-    if(d_rows) rows = min(rows, (long long)*d_rows);
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     const long long warp = ((long long)blockIdx.x * IBLK + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * IBLK) >> 5;
@@ -214,8 +210,8 @@ __global__ void __launch_bounds__(IBLK) k_mlp_infer(MlpDev m, const uint4* __res
         float ylo, yhi, a3[8][4];
         forward_tile<false>(s, ax, g, t, nullptr, nullptr, ylo, yhi, a3);
         if(t == 0) {
-            if(rl < rows) y[scatter ? (long long)feat[rl].w : rl] = ylo;
-            if(rh < rows) y[scatter ? (long long)feat[rh].w : rh] = yhi;
+            if(rl < rows) y[rl] = ylo;
+            if(rh < rows) y[rh] = yhi;
         }
     }
 }
@@ -487,13 +483,11 @@ MlpDev mlp_device(sphgpu_ctx* c)
     return m;
 }
 
-int mlp_infer_pairs(sphgpu_ctx* c, const unsigned long long* d_rows, long long max_rows)
+int mlp_infer_rows(sphgpu_ctx* c, const uint4* feat, float* y, long long rows)
 {
-    // persistent grid: the row count is only known on the device
-    const long long tiles = (max_rows + 15) / 16;
-    const long long blocks = std::min<long long>((tiles + (IBLK / 32) - 1) / (IBLK / 32), 148LL * 8);
-    k_mlp_infer<<<(unsigned)std::max<long long>(blocks, 1), IBLK, 0, c->stream>>>(mlp_device(c), c->d_mlp_feat,
-                                                                                c->d_mlp_y, max_rows, d_rows, true);
+    const long long tiles = (rows + 15) / 16;
+    const long long blocks = std::min<long long>((tiles + (IBLK / 32) - 1) / (IBLK / 32), 148LL * 16);
+    k_mlp_infer<<<(unsigned)std::max<long long>(blocks, 1), IBLK, 0, c->stream>>>(mlp_device(c), feat, y, rows);
     SPHGPU_LAUNCH_CHECK(c, "MLP inference");
     return SPHGPU_OK;
 }
@@ -506,8 +500,7 @@ int mlp_predict_states(sphgpu_ctx* c, const double* d_states, long long n, float
     k_state_features<<<grid_for(n, 256), 256, 0, c->stream>>>(d_states, nullptr, n, feat, nullptr);
     const long long tiles = (n + 15) / 16;
     const long long blocks = std::min<long long>((tiles + 3) / 4, 148LL * 16);
-    k_mlp_infer<<<(unsigned)std::max<long long>(blocks, 1), IBLK, 0, c->stream>>>(mlp_device(c), feat, d_y, n, nullptr,
-                                                                                false);
+    k_mlp_infer<<<(unsigned)std::max<long long>(blocks, 1), IBLK, 0, c->stream>>>(mlp_device(c), feat, d_y, n);
     SPHGPU_LAUNCH_CHECK(c, "MLP predict");
     SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
     cudaFree(feat);
@@ -618,7 +611,7 @@ int sphgpu_mlp_predict(sphgpu_ctx* c, const double* states, int64_t n, float* y)
     SPHGPU_CUDA(c, cudaMalloc(&d_y, sizeof(float) * (size_t)n));
     const long long tiles = (n + 15) / 16;
     const long long blocks = std::min<long long>((tiles + 3) / 4, 148LL * 16);
-    k_mlp_infer<<<(unsigned)blocks, IBLK, 0, c->stream>>>(mlp_device(c), feat, d_y, n, nullptr, false);
+    k_mlp_infer<<<(unsigned)blocks, IBLK, 0, c->stream>>>(mlp_device(c), feat, d_y, n);
     SPHGPU_LAUNCH_CHECK(c, "MLP predict");
     SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));  // the context stream does not sync with cudaMemcpy
     SPHGPU_CUDA(c, cudaMemcpy(y, d_y, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost));

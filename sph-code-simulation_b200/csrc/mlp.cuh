@@ -9,6 +9,7 @@
 // x2/5, min(x3, 64)/8, (gamma - 1.5) * 4) so every input is O(1).
 #pragma once
 
+#include <cstdint>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -64,13 +65,21 @@ __device__ __forceinline__ void mlp_features(const double* L, const double* R, d
     x[4] = (float)((gamma - 1.5) * 4.0);
 }
 
-// Buffers of the learned path: compacted feature rows (8 bf16, 5 used; .w =
-// the pair slot i*cap + k) for the pairs the screen sends to the network, the
-// row count, and per pair slot the network output log(p_star / p_L).
+// Buffers of the learned path.  The force pass appends a row per pair whose
+// linearised start the screen rejects (features: 8 bf16, 5 used; key: the pair
+// slot i*cap + k), up to rcap rows; the network writes y[row] = log(p_star /
+// p_L); after a sort by key, dstart/dcount give each particle's deferred rows,
+// which the completion pass finishes in key order.
 struct MlpPairs {
     uint4* feat;
-    const float* y;
+    uint64_t* keys;
     unsigned long long* rows;
+    long long rcap;
+    const float* y;
+    const uint64_t* skeys;    // sorted keys
+    const uint32_t* svals;    // row of each sorted key
+    const int* dstart;
+    const int* dcount;
 };
 
 // Sampled pair states written by the plain solver (training data): records
@@ -83,7 +92,7 @@ struct Harvest {
     unsigned salt;
 };
 // Launchers (mlp.cu).
-int mlp_infer_pairs(sphgpu_ctx* c, const unsigned long long* d_rows, long long max_rows);
+int mlp_infer_rows(sphgpu_ctx* c, const uint4* feat, float* y, long long rows);
 int mlp_predict_states(sphgpu_ctx* c, const double* d_states, long long n, float* d_y);
 
 __device__ __forceinline__ unsigned pack_bf16x2(float lo, float hi)

@@ -87,8 +87,9 @@ def test_gsph_force_with_learned_guess(gpu):
     p = gpu.config_params("tube_gsph", range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.1, 0.1))
     fields = gpu.sample_shock_tube(0.02, ly=0.1)
     out = {}
-    for guess in (gpu.GUESS_NONE, gpu.GUESS_MLP):
-        p.riemann_guess = guess
+    weights = None
+    for guess in (gpu.GUESS_NONE, gpu.GUESS_MLP, "rerun"):
+        p.riemann_guess = gpu.GUESS_NONE if guess == gpu.GUESS_NONE else gpu.GUESS_MLP
         with gpu.Simulation(p) as sim:
             if guess == gpu.GUESS_MLP:
                 import mlp_oracle as M
@@ -97,6 +98,9 @@ def test_gsph_force_with_learned_guess(gpu):
                 keep = pl > 1e-20
                 sim.mlp_init(1)
                 sim.mlp_train(st[keep], pl[keep], epochs=4, batch=8192)
+                weights = sim.mlp_get_params()
+            elif guess == "rerun":
+                sim.mlp_set_params(weights)
             sim.upload(fields)
             sim.initialize()
             sim.integrate()
@@ -107,6 +111,13 @@ def test_gsph_force_with_learned_guess(gpu):
     for k in "xyz":
         assert np.max(np.abs(a1["acc_" + k] - a0["acc_" + k])) / amax < 1e-4
     assert c1["riemann_solves"] == c0["riemann_solves"]
+    assert c1["mlp_guesses"] > 0
+    # deferred pairs complete in pair-slot order: a second context with the
+    # same weights gives bit-identical results
+    a2, c2 = out["rerun"]
+    for k in ("acc_x", "acc_y", "acc_z", "ene", "vel_x", "pos_x"):
+        np.testing.assert_array_equal(a2[k], a1[k], err_msg=k)
+    assert c2["mlp_guesses"] == c1["mlp_guesses"]
 
 
 def test_harvest_pair_states(gpu):
