@@ -383,6 +383,7 @@ int sphgpu_destroy(sphgpu_ctx* c)
     if(c->d_mlp) cudaFree(c->d_mlp);
     if(c->d_mlp_master) cudaFree(c->d_mlp_master);
     if(c->d_relax) cudaFree(c->d_relax);
+    if(c->d_gnode) cudaFree(c->d_gnode);
     if(c->d_mlp_defer) cudaFree(c->d_mlp_defer);
     if(c->d_harvest) cudaFree(c->d_harvest);
     if(c->d_harvest_count) cudaFree(c->d_harvest_count);

@@ -66,6 +66,9 @@ struct sphgpu_ctx {
     void* d_mlp_defer = nullptr;
     int64_t mlp_rcap = 0;             // rows the allocation holds
     int64_t mlp_ncap = 0;             // particles the allocation holds
+    // mixed-precision gravity: 32-byte FP32 node records of the current tree
+    void* d_gnode = nullptr;
+    int gnode_cap = 0;
     bool have_mlp = false;
     std::vector<float> mlp_master;
     // pair-state harvesting (training data from the plain solver's own runs)
@@ -129,6 +132,10 @@ int exhaustive_lists(sphgpu_ctx* c, int is_ij, int64_t* offsets, int32_t* ids, i
 int pre_interaction(sphgpu_ctx* c);
 int fluid_force(sphgpu_ctx* c);
 int gravity(sphgpu_ctx* c, bool direct);
+// Mixed-precision Barnes-Hut walk: FP32 node records of the current tree,
+// then the walk (one launch each).
+int gravity_nodes_mixed(sphgpu_ctx* c);
+int gravity_walk_mixed(sphgpu_ctx* c);
 int timestep(sphgpu_ctx* c);
 int predict(sphgpu_ctx* c);
 int correct(sphgpu_ctx* c);

@@ -16,12 +16,12 @@
 // exactly the order of the reference's recursion and adds into acc (starting
 // from the fluid acceleration) in that order, so in the plain form with
 // unfused FP64 (-fmad=false for this file) the result is bit-identical to the
-// reference's on the same tree.
-// T = float (mixed form): distances, opening test and kernels in FP32, the
-// per-particle acc / phi accumulators in FP64.
+// reference's on the same tree.  The mixed-precision walk is in
+// gravity_mixed.cu (compiled with FMA contraction).
 #include <cuda_runtime.h>
 
 #include "context.cuh"
+#include "softening.cuh"
 
 namespace sphgpu {
 
@@ -29,32 +29,6 @@ namespace {
 
 constexpr int GBLK = 128;
 
-// Hernquist & Katz (1989) potential / force kernels (src/bhtree.cpp:318-345)
-template <typename T>
-__device__ __forceinline__ T hk_f(T r, T h)
-{
-    const T e = h * T(0.5);
-    const T u = r / e;
-    if(u < T(1.0)) return (T(-0.5) * u * u * (T(1.0 / 3.0) - T(3.0 / 20) * u * u + u * u * u / T(20)) + T(1.4)) / e;
-    if(u < T(2.0))
-        return T(-1.0) / (T(15) * r) + (-u * u * (T(4.0 / 3.0) - u + T(0.3) * u * u - u * u * u / T(30)) + T(1.6)) / e;
-    return T(1) / r;
-}
-
-template <typename T>
-__device__ __forceinline__ T hk_g(T r, T h)
-{
-    const T e = h * T(0.5);
-    const T u = r / e;
-    if(u < T(1.0)) return (T(4.0 / 3.0) - T(1.2) * u * u + T(0.5) * u * u * u) / (e * e * e);
-    if(u < T(2.0))
-        return (T(-1.0 / 15) + T(8.0 / 3) * u * u * u - T(3) * u * u * u * u + T(1.2) * u * u * u * u * u
-                - u * u * u * u * u * u / T(6.0))
-            / (r * r * r);
-    return T(1) / (r * r * r);
-}
-
-template <typename T>
 __global__ void __launch_bounds__(GBLK) k_gravity(DevParams P, DevState S, DevTree Tr, int n,
                                                   DevStatus* __restrict__ st)
 {
@@ -72,7 +46,6 @@ __global__ void __launch_bounds__(GBLK) k_gravity(DevParams P, DevState S, DevTr
     }
     double ax = acc.x, ay = acc.y, az = acc.z, phi = 0.0;
     const double G = P.G;
-    const T theta2 = (T)P.theta2;
     const int nnodes = *Tr.nnodes;
     // node edges halve exactly per level: edge(L) = root edge * 2^(1 - L)
     const double root_edge = ldg4(&Tr.geo[0]).w;
@@ -89,32 +62,16 @@ __global__ void __launch_bounds__(GBLK) k_gravity(DevParams P, DevState S, DevTr
             const double edge = ldexp(root_edge, 1 - (lk.w & 0xff));
             const double4 mc = ldg4(&Tr.mass[nd]);
             const Vec3d d = rij(P, xi, yi, zi, mc.x, mc.y, mc.z);
-            if(sizeof(T) == sizeof(double)) {
-                const double l2 = edge * edge;
-                const double d2 = d.x * d.x + d.y * d.y + d.z * d.z;
-                open = (l2 > P.theta2 * d2) || (d2 < l2);
-                if(!open) {
-                    const double rinv = 1.0 / sqrt(d2);
-                    phi -= G * mc.w * rinv;
-                    const double s = G * mc.w * (rinv * rinv * rinv);
-                    ax -= d.x * s;
-                    ay -= d.y * s;
-                    az -= d.z * s;
-                }
-            } else {
-                const float dx = (float)d.x, dy = (float)d.y, dz = (float)d.z;
-                const float l2 = (float)edge * (float)edge;
-                const float d2 = dx * dx + dy * dy + dz * dz;
-                open = (l2 > (float)theta2 * d2) || (d2 < l2);
-                if(!open) {
-                    const float rinv = rsqrtf(d2);
-                    const float gm = (float)(G * mc.w);
-                    phi -= (double)(gm * rinv);
-                    const float s = gm * (rinv * rinv * rinv);
-                    ax -= (double)(dx * s);
-                    ay -= (double)(dy * s);
-                    az -= (double)(dz * s);
-                }
+            const double l2 = edge * edge;
+            const double d2 = d.x * d.x + d.y * d.y + d.z * d.z;
+            open = (l2 > P.theta2 * d2) || (d2 < l2);
+            if(!open) {
+                const double rinv = 1.0 / sqrt(d2);
+                phi -= G * mc.w * rinv;
+                const double s = G * mc.w * (rinv * rinv * rinv);
+                ax -= d.x * s;
+                ay -= d.y * s;
+                az -= d.z * s;
             }
             if(open && leaf) {
                 for(int q = lk.x; q < lk.y; ++q) {
@@ -122,23 +79,12 @@ __global__ void __launch_bounds__(GBLK) k_gravity(DevParams P, DevState S, DevTr
                     const double4 pq = ldg4(&S.pos[q]);
                     const double hq = ldg4(&S.vel[q]).w;
                     const Vec3d r = rij(P, xi, yi, zi, pq.x, pq.y, pq.z);
-                    if(sizeof(T) == sizeof(double)) {
-                        const double rr = sqrt(r.x * r.x + r.y * r.y + r.z * r.z);
-                        phi -= G * pq.w * (hk_f<double>(rr, hi) + hk_f<double>(rr, hq)) * 0.5;
-                        const double c = G * pq.w * (hk_g<double>(rr, hi) + hk_g<double>(rr, hq)) * 0.5;
-                        ax -= r.x * c;
-                        ay -= r.y * c;
-                        az -= r.z * c;
-                    } else {
-                        const float rx = (float)r.x, ry = (float)r.y, rz = (float)r.z;
-                        const float rr = sqrtf(rx * rx + ry * ry + rz * rz);
-                        const float gm = (float)(G * pq.w);
-                        phi -= (double)(gm * (hk_f<float>(rr, (float)hi) + hk_f<float>(rr, (float)hq)) * 0.5f);
-                        const float c = gm * (hk_g<float>(rr, (float)hi) + hk_g<float>(rr, (float)hq)) * 0.5f;
-                        ax -= (double)(rx * c);
-                        ay -= (double)(ry * c);
-                        az -= (double)(rz * c);
-                    }
+                    const double rr = sqrt(r.x * r.x + r.y * r.y + r.z * r.z);
+                    phi -= G * pq.w * (hk_f<double>(rr, hi) + hk_f<double>(rr, hq)) * 0.5;
+                    const double c = G * pq.w * (hk_g<double>(rr, hi) + hk_g<double>(rr, hq)) * 0.5;
+                    ax -= r.x * c;
+                    ay -= r.y * c;
+                    az -= r.z * c;
                 }
             }
         }
@@ -186,13 +132,21 @@ int gravity(sphgpu_ctx* c, bool direct)
 {
     if(!c->prm.use_gravity) return SPHGPU_OK;
     if(!direct && !c->have_tree) return fail(c, SPHGPU_ERR_STATE, "GravityForce before tree make");
+    if(!direct && c->prm.precision == SPHGPU_MIXED) {
+        // the walk's FP32 node records: tree data, timed with the tree
+        stage_begin(c, SPHGPU_T_TREE);
+        const int rc = gravity_nodes_mixed(c);
+        if(rc < 0) return rc;
+        stage_end(c, SPHGPU_T_TREE, 1);
+    }
     stage_begin(c, SPHGPU_T_GRAVITY);
     if(direct) {
         k_gravity_direct<<<grid_for(c->n, 128), 128, 0, c->stream>>>(c->dp, c->s, c->n, c->d_inv);
     } else if(c->prm.precision == SPHGPU_MIXED) {
-        k_gravity<float><<<grid_for(c->n, GBLK), GBLK, 0, c->stream>>>(c->dp, c->s, c->t, c->n, c->d_status);
+        const int rc = gravity_walk_mixed(c);
+        if(rc < 0) return rc;
     } else {
-        k_gravity<double><<<grid_for(c->n, GBLK), GBLK, 0, c->stream>>>(c->dp, c->s, c->t, c->n, c->d_status);
+        k_gravity<<<grid_for(c->n, GBLK), GBLK, 0, c->stream>>>(c->dp, c->s, c->t, c->n, c->d_status);
     }
     SPHGPU_LAUNCH_CHECK(c, "GravityForce");
     stage_end(c, SPHGPU_T_GRAVITY, 1);
