@@ -44,7 +44,7 @@ extern "C" {
 
 /* ---- enums: same order as sph::SPHType / KernelType / RiemannSolverType
  *      (include/parameters.hpp:8-31) ---- */
-enum sphgpu_sph_type { SPHGPU_SSPH = 0, SPHGPU_DISPH = 1, SPHGPU_GSPH = 2, SPHGPU_GDISPH = 3 };
+enum sphgpu_sph_type { SPHGPU_SSPH = 0, SPHGPU_DISPH = 1, SPHGPU_GSPH = 2, SPHGPU_GDISPH = 3, SPHGPU_SRGSPH = 4 };
 enum sphgpu_kernel   { SPHGPU_CUBIC_SPLINE = 0, SPHGPU_WENDLAND = 1 };
 enum sphgpu_riemann  { SPHGPU_RIEMANN_HLL = 0, SPHGPU_RIEMANN_ITERATIVE = 1 };
 enum sphgpu_precision { SPHGPU_FP64 = 0, SPHGPU_MIXED = 1 };
@@ -59,7 +59,10 @@ enum sphgpu_status {
     SPHGPU_ERR_NEIGHBOR_OVERFLOW = -3, /* > neighbor_number*1000 neighbours (src/bhtree.cpp:129-135) */
     SPHGPU_ERR_NODE_POOL = -4,     /* more nodes than 5*N+1 (src/bhtree.cpp:222-224) */
     SPHGPU_ERR_STATE = -5,         /* call out of order (e.g. force before tree) */
-    SPHGPU_ERR_NO_MLP = -6         /* riemann_guess = MLP without weights */
+    SPHGPU_ERR_NO_MLP = -6,        /* riemann_guess = MLP without weights */
+    SPHGPU_ERR_SR_RECOVERY = -7    /* srgsph: the Lorentz-factor solve of the primitive
+                                      recovery did not converge (the reference throws
+                                      std::runtime_error, src/srgsph/sr_primitive_recovery.cpp:75) */
 };
 
 /* Subset of sph::SPHParameters (include/parameters.hpp:33-91) that the hot
@@ -95,11 +98,21 @@ typedef struct sphgpu_params {
     int32_t riemann_guess;         /* sphgpu_guess: none / learned MLP      */
     int32_t mlp_max_newton;        /* learned form: Newton iterations before
                                       falling back to the plain solver (4)  */
+    /* SRGSPH (SPHParameters::srgsph, include/parameters.hpp:89-96; keys of
+     * src/solver.cpp:430-438) */
+    int32_t sr_2nd_order;          /* "use2ndOrderSRGSPH" (1)               */
+    double  sr_c_speed;            /* "cSpeed" (1.0)                        */
+    double  sr_c_shock;            /* "cShock" (3.0)                        */
+    double  sr_c_cd;               /* "cContactDiscontinuity" (1.0)         */
+    double  sr_eta;                /* "etaSmoothingLength" (1.0)            */
+    double  sr_c_smooth;           /* "cSmoothGradient" (2.0)               */
 } sphgpu_params;
 
 /* Per-particle fields, in the order of sph::SPHParticle where it has them
  * (include/particle.hpp:8-43), then the GSPH named arrays
- * (src/solver.cpp:707-719). Used by upload/download. */
+ * (src/solver.cpp:707-719), then the SRGSPH particle fields
+ * (include/particle.hpp:31-38: S, e, N, nu, gamma_lor, enthalpy, dS, de; held
+ * on the device only by SRGSPH contexts). Used by upload/download. */
 enum sphgpu_field {
     SPHGPU_F_POS_X = 0, SPHGPU_F_POS_Y, SPHGPU_F_POS_Z,
     SPHGPU_F_VEL_X, SPHGPU_F_VEL_Y, SPHGPU_F_VEL_Z,
@@ -113,6 +126,9 @@ enum sphgpu_field {
     SPHGPU_F_GRAD_V0_X, SPHGPU_F_GRAD_V0_Y, SPHGPU_F_GRAD_V0_Z,
     SPHGPU_F_GRAD_V1_X, SPHGPU_F_GRAD_V1_Y, SPHGPU_F_GRAD_V1_Z,
     SPHGPU_F_GRAD_V2_X, SPHGPU_F_GRAD_V2_Y, SPHGPU_F_GRAD_V2_Z,
+    SPHGPU_F_SR_S_X, SPHGPU_F_SR_S_Y, SPHGPU_F_SR_S_Z, SPHGPU_F_SR_E,
+    SPHGPU_F_SR_N, SPHGPU_F_SR_NU, SPHGPU_F_SR_GAMMA_LOR, SPHGPU_F_SR_ENTHALPY,
+    SPHGPU_F_SR_DS_X, SPHGPU_F_SR_DS_Y, SPHGPU_F_SR_DS_Z, SPHGPU_F_SR_DE,
     SPHGPU_NFIELDS
 };
 
@@ -366,6 +382,9 @@ int64_t sphgpu_sample_shear_layer(double dx, double lz, double gamma, double* co
 /* 3-D shock tube along x in [-0.5, 0.5] x [0, ly]^2. */
 int64_t sphgpu_sample_shock_tube(double dx, double ly, double p_left, double p_right, double gamma,
                                  double* const* fields);
+/* Special-relativistic Sod tube after Solver::make_sr_sod
+   (src/sample/sr_sod.cpp:15-199) in 3-D; ly / (2 dx) a whole number. */
+int64_t sphgpu_sample_sr_shock_tube(double dx, double ly, double gamma, double c_speed, double* const* fields);
 
 #ifdef __cplusplus
 }

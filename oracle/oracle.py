@@ -32,6 +32,8 @@ FIELDS = [
     "grad_d_x", "grad_d_y", "grad_d_z", "grad_p_x", "grad_p_y", "grad_p_z",
     "grad_v0_x", "grad_v0_y", "grad_v0_z", "grad_v1_x", "grad_v1_y", "grad_v1_z",
     "grad_v2_x", "grad_v2_y", "grad_v2_z",
+    "sr_S_x", "sr_S_y", "sr_S_z", "sr_e", "sr_N", "sr_nu", "sr_gamma_lor", "sr_enthalpy",
+    "sr_dS_x", "sr_dS_y", "sr_dS_z", "sr_de",
 ]
 NF = len(FIELDS)
 FI = {f: k for k, f in enumerate(FIELDS)}

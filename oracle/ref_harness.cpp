@@ -39,6 +39,11 @@
 #include "exhaustive_search.hpp"
 #include "exception.hpp"
 #include "relaxation/lane_emden_relaxation.hpp"
+#include "srgsph/sr_pre_interaction.hpp"
+#include "srgsph/sr_fluid_force.hpp"
+#include "srgsph/sr_timestep.hpp"
+#include "srgsph/sr_primitive_recovery.hpp"
+#include <omp.h>
 
 #include <unistd.h>
 
@@ -65,7 +70,8 @@ std::shared_ptr<SPHParameters> to_param(const sphgpu_params* p)
     q->time.end = 1.0;
     q->type = p->sph_type == SPHGPU_DISPH  ? SPHType::DISPH
             : p->sph_type == SPHGPU_GSPH   ? SPHType::GSPH
-            : p->sph_type == SPHGPU_GDISPH ? SPHType::GDISPH : SPHType::SSPH;
+            : p->sph_type == SPHGPU_GDISPH ? SPHType::GDISPH
+            : p->sph_type == SPHGPU_SRGSPH ? SPHType::SRGSPH : SPHType::SSPH;
     q->cfl.sound = p->cfl_sound;
     q->cfl.force = p->cfl_force;
     q->av.alpha = p->av_alpha;
@@ -93,6 +99,12 @@ std::shared_ptr<SPHParameters> to_param(const sphgpu_params* p)
     q->gsph.is_2nd_order = p->gsph_2nd_order != 0;
     q->gsph.riemann_solver = p->riemann_solver == SPHGPU_RIEMANN_ITERATIVE
         ? RiemannSolverType::ITERATIVE : RiemannSolverType::HLL;
+    q->srgsph.is_2nd_order = p->sr_2nd_order != 0;
+    q->srgsph.c_speed = p->sr_c_speed;
+    q->srgsph.c_shock = p->sr_c_shock;
+    q->srgsph.c_cd = p->sr_c_cd;
+    q->srgsph.eta = p->sr_eta;
+    q->srgsph.c_smooth = p->sr_c_smooth;
     return q;
 }
 
@@ -101,9 +113,64 @@ double now()
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+void store_prim(const RefCtx& c, SPHParticle& p, const srgsph::PrimitiveVariables& q)
+{
+    const real gamma = c.param->physics.gamma;
+    p.vel = q.vel;
+    p.ene = q.pressure / ((gamma - 1.0) * q.density);
+    p.pres = q.pressure;
+    p.dens = q.density;
+    p.sound = q.sound_speed;
+    p.gamma_lor = q.gamma_lor;
+    p.enthalpy = q.enthalpy;
+}
+
+// Solver::predict, SRGSPH branch (src/solver.cpp:992-1043; diagnostics left out).
+void predict_sr(RefCtx& c)
+{
+    auto& p = c.sim->get_particles();
+    const int num = c.sim->get_particle_num();
+    auto* periodic = c.sim->get_periodic().get();
+    const real dt = c.sim->get_dt();
+    const real gamma = c.param->physics.gamma;
+    const real c_speed = c.param->srgsph.c_speed;
+    for(int i = 0; i < num; ++i) {
+        vec_t S_half = p[i].S + p[i].dS * (0.5 * dt);
+        real e_half = p[i].e + p[i].de * (0.5 * dt);
+        p[i].S += p[i].dS * dt;
+        p[i].e += p[i].de * dt;
+        auto prim_half = srgsph::PrimitiveRecovery::conserved_to_primitive(S_half, e_half, p[i].N, gamma, c_speed);
+        p[i].pos += prim_half.vel * dt;
+        periodic->apply(p[i].pos);
+        auto prim_full = srgsph::PrimitiveRecovery::conserved_to_primitive(p[i].S, p[i].e, p[i].N, gamma, c_speed);
+        store_prim(c, p[i], prim_full);
+        p[i].vel_p = prim_half.vel;
+        p[i].ene_p = prim_half.pressure / ((gamma - 1.0) * prim_half.density);
+    }
+}
+
+// Solver::correct, SRGSPH branch (src/solver.cpp:1075-1102).
+void correct_sr(RefCtx& c)
+{
+    auto& p = c.sim->get_particles();
+    const int num = c.sim->get_particle_num();
+    const real dt = c.sim->get_dt();
+    const real gamma = c.param->physics.gamma;
+    const real c_speed = c.param->srgsph.c_speed;
+    for(int i = 0; i < num; ++i) {
+        vec_t S_half = p[i].S - p[i].dS * (0.5 * dt);
+        real e_half = p[i].e - p[i].de * (0.5 * dt);
+        p[i].S = S_half + p[i].dS * (0.5 * dt);
+        p[i].e = e_half + p[i].de * (0.5 * dt);
+        auto prim = srgsph::PrimitiveRecovery::conserved_to_primitive(p[i].S, p[i].e, p[i].N, gamma, c_speed);
+        store_prim(c, p[i], prim);
+    }
+}
+
 // Solver::predict (src/solver.cpp:1046-1061), non-relativistic branch.
 void predict(RefCtx& c)
 {
+    if(c.param->type == SPHType::SRGSPH) return predict_sr(c);
     auto& p = c.sim->get_particles();
     const int num = c.sim->get_particle_num();
     auto* periodic = c.sim->get_periodic().get();
@@ -125,6 +192,7 @@ void predict(RefCtx& c)
 // Solver::correct (src/solver.cpp:1104-1112), non-relativistic branch.
 void correct(RefCtx& c)
 {
+    if(c.param->type == SPHType::SRGSPH) return correct_sr(c);
     auto& p = c.sim->get_particles();
     const int num = c.sim->get_particle_num();
     const real dt = c.sim->get_dt();
@@ -180,6 +248,18 @@ double* field_ptr(SPHParticle& p, int k)
     case SPHGPU_F_ALPHA: return &p.alpha;
     case SPHGPU_F_GRADH: return &p.gradh;
     case SPHGPU_F_PHI: return &p.phi;
+    case SPHGPU_F_SR_S_X: return &p.S[0];
+    case SPHGPU_F_SR_S_Y: return &p.S[1];
+    case SPHGPU_F_SR_S_Z: return &p.S[2];
+    case SPHGPU_F_SR_E: return &p.e;
+    case SPHGPU_F_SR_N: return &p.N;
+    case SPHGPU_F_SR_NU: return &p.nu;
+    case SPHGPU_F_SR_GAMMA_LOR: return &p.gamma_lor;
+    case SPHGPU_F_SR_ENTHALPY: return &p.enthalpy;
+    case SPHGPU_F_SR_DS_X: return &p.dS[0];
+    case SPHGPU_F_SR_DS_Y: return &p.dS[1];
+    case SPHGPU_F_SR_DS_Z: return &p.dS[2];
+    case SPHGPU_F_SR_DE: return &p.de;
     default: return nullptr;
     }
 }
@@ -199,7 +279,7 @@ void* ref_create(const sphgpu_params* p, int64_t n, const double* const* fields)
     c->sim = std::make_shared<Simulation>(c->param);
     std::vector<SPHParticle> parts(n);
     for(int64_t i = 0; i < n; ++i) {
-        for(int k = 0; k < SPHGPU_F_NEIGHBOR; ++k) {
+        for(int k = 0; k < SPHGPU_NFIELDS; ++k) {
             double* d = field_ptr(parts[i], k);
             if(d) *d = fields && fields[k] ? fields[k][i] : 0.0;
         }
@@ -222,6 +302,16 @@ void* ref_create(const sphgpu_params* p, int64_t n, const double* const* fields)
         c->fforce = std::make_shared<gdisph::FluidForce>();
         std::vector<std::string> names(grad_names, grad_names + 5);
         c->sim->add_vector_array(names);
+    } else if(c->param->type == SPHType::SRGSPH) {
+        // src/solver.cpp:699-719; the pre-interaction's particle loop reads
+        // neighbours' N while it updates its own, so the harness runs it on
+        // one thread (index order)
+        c->timestep = std::make_shared<srgsph::TimeStep>();
+        c->pre = std::make_shared<srgsph::PreInteraction>();
+        c->fforce = std::make_shared<srgsph::FluidForce>();
+        std::vector<std::string> names(grad_names, grad_names + 5);
+        c->sim->add_vector_array(names);
+        omp_set_num_threads(1);
     } else {
         c->pre = std::make_shared<PreInteraction>();
         c->fforce = std::make_shared<FluidForce>();
@@ -250,7 +340,11 @@ int ref_get(void* h, double* const* fields)
         }
         if(fields[SPHGPU_F_NEIGHBOR]) fields[SPHGPU_F_NEIGHBOR][i] = parts[i].neighbor;
     }
-    if(c->param->type == SPHType::GSPH || c->param->type == SPHType::GDISPH) {
+    for(int k = SPHGPU_F_SR_S_X; k < SPHGPU_NFIELDS; ++k) {
+        if(!fields[k]) continue;
+        for(int i = 0; i < n; ++i) fields[k][i] = *field_ptr(parts[i], k);
+    }
+    if(c->param->type == SPHType::GSPH || c->param->type == SPHType::GDISPH || c->param->type == SPHType::SRGSPH) {
         for(int g = 0; g < 5; ++g) {
             auto& arr = c->sim->get_vector_array(grad_names[g]);
             for(int d = 0; d < 3; ++d) {
@@ -269,8 +363,9 @@ int ref_set(void* h, const double* const* fields)
     auto& parts = c->sim->get_particles();
     const int n = c->sim->get_particle_num();
     for(int i = 0; i < n; ++i) {
-        for(int k = 0; k < SPHGPU_F_NEIGHBOR; ++k) {
-            if(fields[k]) *field_ptr(parts[i], k) = fields[k][i];
+        for(int k = 0; k < SPHGPU_NFIELDS; ++k) {
+            double* d = field_ptr(parts[i], k);
+            if(d && fields[k]) *d = fields[k][i];
         }
     }
     return 0;

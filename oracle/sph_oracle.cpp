@@ -485,6 +485,7 @@ struct Oracle {
     real time = 0.0, dt = 0.0, h_per_v_sig = 0.0;
     bool first_pre = true;
     bool exhaustive = false;  // -DEXHAUSTIVE_SEARCH behaviour
+    bool sr_failed = false;   // a primitive recovery in predict / correct did not converge
     int64_t newton_nonconv = 0, riemann_solves = 0, riemann_iters = 0;
     std::string err;
 
@@ -585,6 +586,7 @@ struct Oracle {
     // density and pressure, the gsph gradients, its own AV switches).
     bool pre_interaction()
     {
+        if(prm.sph_type == SPHGPU_SRGSPH) return sr_pre();
         if(first_pre) {
             if(!initial_smoothing()) return false;
             first_pre = false;
@@ -765,6 +767,7 @@ struct Oracle {
     // and HLL star pressure inside the disph pressure-energy terms)
     bool fluid_force()
     {
+        if(prm.sph_type == SPHGPU_SRGSPH) return sr_force();
         const int type = prm.sph_type;
         bool ok = true;
         int64_t solves = 0, iters = 0;
@@ -960,6 +963,7 @@ struct Oracle {
     // TimeStep::calculation (src/timestep.cpp:18-38)
     void timestep()
     {
+        if(prm.sph_type == SPHGPU_SRGSPH) return sr_timestep();
         real dtmin = std::numeric_limits<real>::max();
         for(int i = 0; i < s.n; ++i) {
             const real a = norm(s.acc(i));
@@ -974,6 +978,7 @@ struct Oracle {
     // Solver::predict (src/solver.cpp:1046-1061)
     void predict()
     {
+        if(prm.sph_type == SPHGPU_SRGSPH) return sr_predict();
         const real cs = prm.gamma * (prm.gamma - 1.0);
         for(int i = 0; i < s.n; ++i) {
             for(int k = 0; k < 3; ++k) {
@@ -996,6 +1001,7 @@ struct Oracle {
     // Solver::correct (src/solver.cpp:1104-1112)
     void correct()
     {
+        if(prm.sph_type == SPHGPU_SRGSPH) return sr_correct();
         const real cs = prm.gamma * (prm.gamma - 1.0);
         for(int i = 0; i < s.n; ++i) {
             for(int k = 0; k < 3; ++k) {
@@ -1003,6 +1009,440 @@ struct Oracle {
             }
             s.f[SPHGPU_F_ENE][i] = s.f[SPHGPU_F_ENE_P][i] + s.f[SPHGPU_F_DENE][i] * (0.5 * dt);
             s.f[SPHGPU_F_SOUND][i] = std::sqrt(cs * s.f[SPHGPU_F_ENE][i]);
+        }
+    }
+
+    // ------------------------------------------------------------ SRGSPH
+    // Special-relativistic GSPH (src/srgsph/*.cpp; Kitajima, Inutsuka & Seno
+    // 2025).  Conserved state per particle: S (canonical momentum), e
+    // (canonical energy), N (lab-frame baryon density), nu (baryons); the
+    // primitives follow from PrimitiveRecovery.
+    struct SRPrim {
+        V3 vel;
+        real density, pressure, sound, enthalpy, gamma_lor;
+    };
+
+    V3 sr_S(int i) const { return {s.f[SPHGPU_F_SR_S_X][i], s.f[SPHGPU_F_SR_S_Y][i], s.f[SPHGPU_F_SR_S_Z][i]}; }
+    V3 sr_dS(int i) const { return {s.f[SPHGPU_F_SR_DS_X][i], s.f[SPHGPU_F_SR_DS_Y][i], s.f[SPHGPU_F_SR_DS_Z][i]}; }
+
+    // PrimitiveRecovery::solve_lorentz_factor (src/srgsph/sr_primitive_recovery.cpp:23-76):
+    // Newton on (g^2-1)(X e g - 1)^2 - S^2 (X g^2 - 1)^2 / c^2 = 0, X = G/(G-1).
+    bool sr_lorentz(real S_mag, real e, real& g) const
+    {
+        const real ge = prm.gamma, c = prm.sr_c_speed;
+        const real X = ge / (ge - 1.0);
+        const real c2 = c * c;
+        const real S2 = S_mag * S_mag;
+        g = 1.0 + std::sqrt(1.0 + S2 / c2) / X;
+        for(int it = 0; it < 100; ++it) {
+            const real g2 = g * g;
+            const real g2m1 = g2 - 1.0;
+            const real xe = X * e * g - 1.0;
+            const real xg = X * g2 - 1.0;
+            const real f = g2m1 * xe * xe - S2 * xg * xg / c2;
+            const real df = 2.0 * g * xe * xe + 2.0 * g2m1 * xe * X * e - 2.0 * S2 * xg * 2.0 * X * g / c2;
+            const real delta = f / df;
+            g -= delta;
+            if(g < 1.0) g = 1.0 + 1.0e-10;
+            if(std::abs(delta) < 1.0e-10 * g) return true;
+        }
+        return false;
+    }
+
+    // PrimitiveRecovery::conserved_to_primitive (src/srgsph/sr_primitive_recovery.cpp:82-160)
+    bool sr_c2p(V3 S, real e, real N, SRPrim& o) const
+    {
+        const real ge = prm.gamma, c = prm.sr_c_speed;
+        const real S_mag = norm(S);
+        if(!sr_lorentz(S_mag, e, o.gamma_lor)) return false;
+        const real X = ge / (ge - 1.0);
+        const real g = o.gamma_lor, g2 = g * g;
+        const real num = X * g2 - 1.0;
+        const real den = g * (X * e * g - 1.0);
+        o.vel = S * (num / den);
+        o.density = N / g;
+        const real v_mag = norm(o.vel);
+        const real c2 = c * c;
+        if(v_mag > 1.0e-10) o.enthalpy = S_mag / (g * v_mag);
+        else o.enthalpy = 1.0 + (e - 1.0) / c2;
+        o.pressure = (ge - 1.0) * o.density * c2 * (o.enthalpy - 1.0) / ge;
+        o.sound = std::sqrt((ge - 1.0) * (o.enthalpy - 1.0) / o.enthalpy);
+        return true;
+    }
+
+    // srgsph::PreInteraction::compute_smoothing_length
+    // (src/srgsph/sr_pre_interaction.cpp:103-246): damped fixed point
+    // h <- (h + eta Vp*(C_smooth h)^(1/3)) / 2 over the list members.
+    real sr_smoothing_length(int i, const std::vector<int>& list) const
+    {
+        real h = s.f[SPHGPU_F_SML][i];
+        const V3 ri = s.pos(i);
+        for(int iter = 0; iter < 20; ++iter) {
+            const real hs = prm.sr_c_smooth * h;
+            real sum = 0.0;
+            for(int j : list) {
+                const real r = norm(per.rij(ri, s.pos(j)));
+                if(r < hs) sum += ker.w(r, hs);
+            }
+            sum += ker.w(0.0, hs);
+            if(sum < 1.0e-20) {
+                h *= 1.5;
+                continue;
+            }
+            const real vp = 1.0 / sum;
+            const real hn = prm.sr_eta * std::pow(vp, 1.0 / real(3));
+            const real hd = 0.5 * (h + hn);
+            if(std::abs(hd - h) < 1.0e-6 * h) return hd;
+            h = hd;
+            if(h < 1.0e-10) h = 1.0e-10;
+            if(h > 10.0) h = 10.0;
+        }
+        return h;
+    }
+
+    // srgsph::PreInteraction::calculation (src/srgsph/sr_pre_interaction.cpp:248-407).
+    // The reference updates N inside its particle loop while the same loop
+    // reads the neighbours' N, so the result depends on the loop order; this
+    // restatement runs the loop serially in index order (the reference's
+    // single-thread result).
+    bool sr_pre()
+    {
+        if(first_pre) {
+            // initial_smoothing (src/srgsph/sr_pre_interaction.cpp:31-67)
+            for(int i = 0; i < s.n; ++i)
+                s.f[SPHGPU_F_SML][i] = prm.sr_eta * std::pow(s.f[SPHGPU_F_SR_NU][i] / s.f[SPHGPU_F_SR_N][i], 1.0 / 3);
+            first_pre = false;
+        }
+        std::vector<int> list;
+        for(int i = 0; i < s.n; ++i) {
+            if(!neighbors(i, false, s.f[SPHGPU_F_SML][i], list)) return false;
+            real& sml = s.f[SPHGPU_F_SML][i];
+            const real nu_i = s.f[SPHGPU_F_SR_NU][i];
+            if(prm.iterative_sml) sml = sr_smoothing_length(i, list);
+            else sml = prm.sr_eta * std::pow(nu_i / s.f[SPHGPU_F_SR_N][i], 1.0 / 3);
+            const real h = sml;
+            const V3 ri = s.pos(i);
+            // compute_volume (src/srgsph/sr_pre_interaction.cpp:69-101)
+            real sw = 0.0;
+            for(int j : list) {
+                const real r = norm(per.rij(ri, s.pos(j)));
+                if(r < h) sw += ker.w(r, h);
+            }
+            sw += ker.w(0.0, h);
+            const real vp = 1.0 / sw;
+            s.f[SPHGPU_F_SR_N][i] = nu_i / vp;
+            SRPrim pi;
+            if(!sr_c2p(sr_S(i), s.f[SPHGPU_F_SR_E][i], s.f[SPHGPU_F_SR_N][i], pi)) {
+                err = "Lorentz factor solver did not converge";
+                return false;
+            }
+            s.f[SPHGPU_F_VEL_X][i] = pi.vel.x;
+            s.f[SPHGPU_F_VEL_Y][i] = pi.vel.y;
+            s.f[SPHGPU_F_VEL_Z][i] = pi.vel.z;
+            s.f[SPHGPU_F_PRES][i] = pi.pressure;
+            s.f[SPHGPU_F_DENS][i] = pi.density;
+            s.f[SPHGPU_F_SOUND][i] = pi.sound;
+            s.f[SPHGPU_F_SR_GAMMA_LOR][i] = pi.gamma_lor;
+            s.f[SPHGPU_F_SR_ENTHALPY][i] = pi.enthalpy;
+            V3 gd{0, 0, 0}, gp{0, 0, 0}, gv[3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            real omega = 0.0;
+            for(int j : list) {
+                const V3 r = per.rij(ri, s.pos(j));
+                const real rr = norm(r);
+                if(rr >= h || rr == 0.0) continue;
+                SRPrim pj;
+                if(!sr_c2p(sr_S(j), s.f[SPHGPU_F_SR_E][j], s.f[SPHGPU_F_SR_N][j], pj)) {
+                    err = "Lorentz factor solver did not converge";
+                    return false;
+                }
+                const V3 dw = ker.dw(r, rr, h);
+                const real vol_j = s.f[SPHGPU_F_SR_NU][j] / s.f[SPHGPU_F_SR_N][j];
+                omega += vol_j * ker.w(rr, h);
+                gd = gd + dw * (vol_j * (pj.density - pi.density));
+                gp = gp + dw * (vol_j * (pj.pressure - pi.pressure));
+                gv[0] = gv[0] + dw * (vol_j * (pj.vel.x - pi.vel.x));
+                gv[1] = gv[1] + dw * (vol_j * (pj.vel.y - pi.vel.y));
+                gv[2] = gv[2] + dw * (vol_j * (pj.vel.z - pi.vel.z));
+            }
+            if(omega > 0.0) {
+                const real oi = 1.0 / omega;
+                s.set_grad(0, i, gd * oi);
+                s.set_grad(1, i, gp * oi);
+                for(int k = 0; k < 3; ++k) s.set_grad(2 + k, i, gv[k] * oi);
+            } else {
+                for(int g = 0; g < 5; ++g) s.set_grad(g, i, V3{0, 0, 0});
+            }
+        }
+        return true;
+    }
+
+    // FluidForce::compute_shock_velocity (src/srgsph/sr_fluid_force.cpp:366-420):
+    // Taub adiabat and Rankine-Hugoniot (Pons, Marti & Mueller 2000).
+    real sr_shock_velocity(real p_a, real rho_a, real h_a, real vx_a, real W_a, real p_b, bool left) const
+    {
+        const real ge = prm.gamma;
+        const real dp = p_a - p_b;
+        const real A = 1.0 + (ge - 1.0) * dp / (ge * p_b);
+        const real B = -h_a * dp / (ge * p_b);
+        const real Cc = -h_a * h_a + h_a * dp / rho_a;
+        const real disc = B * B - 4.0 * A * Cc;
+        if(disc < 0.0) return vx_a;
+        const real h_b = (-B + std::sqrt(disc)) / (2.0 * A);
+        const real rho_b = ge * p_b / ((ge - 1.0) * (h_b - 1.0));
+        const real hra = h_a / rho_a;
+        const real hrb = h_b / rho_b;
+        const real j2 = -(p_b - p_a) / (hrb - hra);
+        if(j2 < 0.0) return vx_a;
+        const real j = left ? -std::sqrt(j2) : std::sqrt(j2);
+        const real rwa = rho_a * W_a;
+        const real rwa2 = rwa * rwa;
+        const real numer = rwa2 * vx_a + j * std::sqrt(j2 + rwa2 * (1.0 - vx_a * vx_a));
+        const real denom = rwa2 + j2;
+        const real Vs = numer / denom;
+        const real Ws = 1.0 / std::sqrt(1.0 - Vs * Vs);
+        const real t1 = h_a * W_a * vx_a + Ws * (p_b - p_a) / j + Ws * Vs / (rho_a * W_a);
+        const real t2 = h_a * W_a + (p_b - p_a) / j;
+        return t2 / t1;
+    }
+
+    // FluidForce::compute_rarefaction_velocity (src/srgsph/sr_fluid_force.cpp:436-480):
+    // 100 explicit Euler steps of dv/dp along the isentrope.
+    real sr_rarefaction_velocity(real p_a, real rho_a, real vx_a, real p_b, bool left) const
+    {
+        const real ge = prm.gamma;
+        const real dp = (p_b - p_a) / 100;
+        real p = p_a, vx = vx_a;
+        for(int k = 0; k < 100; ++k) {
+            const real eps = (ge - 1.0) * p / rho_a;
+            const real rho = rho_a * std::pow(p / p_a, 1.0 / ge);
+            const real h = 1.0 + eps + p / rho;
+            const real cs = std::sqrt(ge * p / (rho * h));
+            const real W = 1.0 / std::sqrt(1.0 - vx * vx);
+            const real sign = left ? -1.0 : 1.0;
+            const real dvdp = sign / (rho * h * W * W * cs);
+            vx += dvdp * dp;
+            p += dp;
+            if(vx >= 1.0) vx = 0.99999;
+            if(vx <= -1.0) vx = -0.99999;
+        }
+        return vx;
+    }
+
+    real sr_wave(real p_star, real p_a, real rho_a, real h_a, real vx_a, real W_a, bool left) const
+    {
+        return p_star > p_a ? sr_shock_velocity(p_a, rho_a, h_a, vx_a, W_a, p_star, left)
+                            : sr_rarefaction_velocity(p_a, rho_a, vx_a, p_star, left);
+    }
+
+    // FluidForce::exact_riemann_solver (src/srgsph/sr_fluid_force.cpp:236-350).
+    // state = (v, n, P, c_s)
+    void sr_riemann(const real* L, const real* R, real& pstar, real& vstar) const
+    {
+        const real ge = prm.gamma;
+        const real vL = L[0], nL = L[1], pL = L[2];
+        const real vR = R[0], nR = R[1], pR = R[2];
+        const real hL = 1.0 + ge * pL / ((ge - 1.0) * nL);
+        const real hR = 1.0 + ge * pR / ((ge - 1.0) * nR);
+        const real WL = 1.0 / std::sqrt(1.0 - vL * vL);
+        const real WR = 1.0 / std::sqrt(1.0 - vR * vR);
+        real ps = 0.5 * (pL + pR);
+        for(int it = 0; it < 50; ++it) {
+            const real vLs = sr_wave(ps, pL, nL, hL, vL, WL, true);
+            const real vRs = sr_wave(ps, pR, nR, hR, vR, WR, false);
+            const real f = vRs - vLs;
+            if(std::abs(f) < 1.0e-8) {
+                pstar = ps;
+                vstar = 0.5 * (vLs + vRs);
+                return;
+            }
+            const real dp = ps * 1.0e-6;
+            const real vLp = sr_wave(ps + dp, pL, nL, hL, vL, WL, true);
+            const real vRp = sr_wave(ps + dp, pR, nR, hR, vR, WR, false);
+            const real fp = vRp - vLp;
+            const real df = (fp - f) / dp;
+            if(std::abs(df) > 1.0e-12) {
+                real pn = ps - 0.5 * f / df;
+                pn = std::max(pn, 0.01 * std::min(pL, pR));
+                ps = pn;
+            } else if(f > 0) {
+                ps *= 0.9;
+            } else {
+                ps *= 1.1;
+            }
+        }
+        const real vLs = sr_wave(ps, pL, nL, hL, vL, WL, true);
+        const real vRs = sr_wave(ps, pR, nR, hR, vR, WR, false);
+        pstar = ps;
+        vstar = 0.5 * (vLs + vRs);
+    }
+
+    // srgsph::FluidForce::calculation (src/srgsph/sr_fluid_force.cpp:47-232)
+    bool sr_force()
+    {
+        bool ok = true;
+        const real ge = prm.gamma;
+#pragma omp parallel for schedule(dynamic, 64)
+        for(int i = 0; i < s.n; ++i) {
+            std::vector<int> list;
+            if(!neighbors(i, true, s.f[SPHGPU_F_SML][i], list)) {
+                ok = false;
+                continue;
+            }
+            const V3 ri = s.pos(i), vi = s.vel(i);
+            const real hi = s.f[SPHGPU_F_SML][i], nu_i = s.f[SPHGPU_F_SR_NU][i];
+            const real ci = s.f[SPHGPU_F_SOUND][i], Pi = s.f[SPHGPU_F_PRES][i];
+            const real Ni = s.f[SPHGPU_F_SR_N][i], gi = s.f[SPHGPU_F_SR_GAMMA_LOR][i];
+            V3 dS{0, 0, 0};
+            real de = 0.0;
+            for(int j : list) {
+                const V3 r = per.rij(ri, s.pos(j));
+                const real rr = norm(r);
+                const real hj = s.f[SPHGPU_F_SML][j];
+                if(rr >= std::max(hi, hj) || rr == 0.0) continue;
+                const real rinv = 1.0 / rr;
+                const V3 e = r * rinv;
+                const V3 vj = s.vel(j);
+                const real vei = dot(vi, e), vej = dot(vj, e);
+                const real cj = s.f[SPHGPU_F_SOUND][j], Pj = s.f[SPHGPU_F_PRES][j];
+                const real Nj = s.f[SPHGPU_F_SR_N][j], gj = s.f[SPHGPU_F_SR_GAMMA_LOR][j];
+                const real n_i = Ni / gi, n_j = Nj / gj;
+                real right[4], left[4], pstar, vstar;
+                bool first = !prm.sr_2nd_order;
+                if(prm.sr_2nd_order) {
+                    const real di = 0.5 * (1.0 - ci * dt * rinv);
+                    const real dj = 0.5 * (1.0 - cj * dt * rinv);
+                    const real dv = vei - vej;
+                    const V3 dvi{dot(s.grad(2, i), e), dot(s.grad(3, i), e), dot(s.grad(4, i), e)};
+                    const V3 dvj{dot(s.grad(2, j), e), dot(s.grad(3, j), e), dot(s.grad(4, j), e)};
+                    const real dve_i = dot(dvi, e) * rr;
+                    const real dve_j = dot(dvj, e) * rr;
+                    const real min_cs = std::min(ci, cj);
+                    const real shock = prm.sr_c_shock * std::abs(vei - vej);
+                    const real pjump = std::abs(std::log10(Pi / Pj));
+                    if((shock > min_cs) || (pjump > prm.sr_c_cd)) {
+                        first = true;
+                    } else {
+                        right[0] = vei - limiter(dv, dve_i) * di;
+                        left[0] = vej + limiter(dv, dve_j) * dj;
+                        const real dn = n_i - n_j;
+                        const real dn_i = dot(s.grad(0, i), e) * rr / gi;
+                        const real dn_j = dot(s.grad(0, j), e) * rr / gj;
+                        right[1] = n_i - limiter(dn, dn_i) * di;
+                        left[1] = n_j + limiter(dn, dn_j) * dj;
+                        const real dpp = Pi - Pj;
+                        const real dp_i = dot(s.grad(1, i), e) * rr;
+                        const real dp_j = dot(s.grad(1, j), e) * rr;
+                        right[2] = Pi - limiter(dpp, dp_i) * di;
+                        left[2] = Pj + limiter(dpp, dp_j) * dj;
+                        right[3] = std::sqrt(ge * right[2] / right[1]);
+                        left[3] = std::sqrt(ge * left[2] / left[1]);
+                    }
+                }
+                if(first) {
+                    right[0] = vei;
+                    right[1] = n_i;
+                    right[2] = Pi;
+                    right[3] = ci;
+                    left[0] = vej;
+                    left[1] = n_j;
+                    left[2] = Pj;
+                    left[3] = cj;
+                }
+                sr_riemann(left, right, pstar, vstar);
+                const V3 dwi = ker.dw(r, rr, 2.0 * hi);
+                const V3 dwj = ker.dw(r, rr, 2.0 * hj);
+                const V3 dwij = dwi - dwj;
+                const real Vi = nu_i / Ni;
+                const real Vj = s.f[SPHGPU_F_SR_NU][j] / Nj;
+                const real V2 = 0.5 * (Vi * Vi + Vj * Vj);
+                dS = dS - dwij * (pstar * V2);
+                const V3 vij = e * vstar;
+                de -= dot(vij, dwij) * (pstar * V2);
+            }
+            s.f[SPHGPU_F_SR_DS_X][i] = dS.x / nu_i;
+            s.f[SPHGPU_F_SR_DS_Y][i] = dS.y / nu_i;
+            s.f[SPHGPU_F_SR_DS_Z][i] = dS.z / nu_i;
+            s.f[SPHGPU_F_SR_DE][i] = de / nu_i;
+        }
+        return ok;
+    }
+
+    // srgsph::TimeStep::calculation (src/srgsph/sr_timestep.cpp:14-59)
+    void sr_timestep()
+    {
+        real dmin = std::numeric_limits<real>::max();
+        for(int i = 0; i < s.n; ++i) {
+            const real cs = std::max(s.f[SPHGPU_F_SOUND][i], real(1.0e-10));
+            const real d = prm.cfl_sound * s.f[SPHGPU_F_SML][i] / cs;
+            if(d < dmin) dmin = d;
+        }
+        dt = dmin;
+    }
+
+    void sr_store(int i, const SRPrim& q)
+    {
+        s.f[SPHGPU_F_VEL_X][i] = q.vel.x;
+        s.f[SPHGPU_F_VEL_Y][i] = q.vel.y;
+        s.f[SPHGPU_F_VEL_Z][i] = q.vel.z;
+        s.f[SPHGPU_F_ENE][i] = q.pressure / ((prm.gamma - 1.0) * q.density);
+        s.f[SPHGPU_F_PRES][i] = q.pressure;
+        s.f[SPHGPU_F_DENS][i] = q.density;
+        s.f[SPHGPU_F_SOUND][i] = q.sound;
+        s.f[SPHGPU_F_SR_GAMMA_LOR][i] = q.gamma_lor;
+        s.f[SPHGPU_F_SR_ENTHALPY][i] = q.enthalpy;
+    }
+
+    // Solver::predict, SRGSPH branch (src/solver.cpp:992-1043)
+    void sr_predict()
+    {
+        for(int i = 0; i < s.n; ++i) {
+            const V3 S = sr_S(i), dS = sr_dS(i);
+            real& e = s.f[SPHGPU_F_SR_E][i];
+            const real de = s.f[SPHGPU_F_SR_DE][i];
+            const V3 Sh = S + dS * (0.5 * dt);
+            const real eh = e + de * (0.5 * dt);
+            const V3 Sn = S + dS * dt;
+            s.f[SPHGPU_F_SR_S_X][i] = Sn.x;
+            s.f[SPHGPU_F_SR_S_Y][i] = Sn.y;
+            s.f[SPHGPU_F_SR_S_Z][i] = Sn.z;
+            e += de * dt;
+            SRPrim ph, pf;
+            if(!sr_c2p(Sh, eh, s.f[SPHGPU_F_SR_N][i], ph) || !sr_c2p(Sn, e, s.f[SPHGPU_F_SR_N][i], pf)) {
+                sr_failed = true;
+                continue;
+            }
+            s.f[SPHGPU_F_POS_X][i] += ph.vel.x * dt;
+            s.f[SPHGPU_F_POS_Y][i] += ph.vel.y * dt;
+            s.f[SPHGPU_F_POS_Z][i] += ph.vel.z * dt;
+            for(int k = 0; k < 3; ++k) per.apply(s.f[SPHGPU_F_POS_X + k][i], k);
+            sr_store(i, pf);
+            s.f[SPHGPU_F_VELP_X][i] = ph.vel.x;
+            s.f[SPHGPU_F_VELP_Y][i] = ph.vel.y;
+            s.f[SPHGPU_F_VELP_Z][i] = ph.vel.z;
+            s.f[SPHGPU_F_ENE_P][i] = ph.pressure / ((prm.gamma - 1.0) * ph.density);
+        }
+    }
+
+    // Solver::correct, SRGSPH branch (src/solver.cpp:1075-1102)
+    void sr_correct()
+    {
+        for(int i = 0; i < s.n; ++i) {
+            const V3 dS = sr_dS(i);
+            const real de = s.f[SPHGPU_F_SR_DE][i];
+            const V3 Sh = sr_S(i) - dS * (0.5 * dt);
+            const real eh = s.f[SPHGPU_F_SR_E][i] - de * (0.5 * dt);
+            const V3 S = Sh + dS * (0.5 * dt);
+            const real e = eh + de * (0.5 * dt);
+            s.f[SPHGPU_F_SR_S_X][i] = S.x;
+            s.f[SPHGPU_F_SR_S_Y][i] = S.y;
+            s.f[SPHGPU_F_SR_S_Z][i] = S.z;
+            s.f[SPHGPU_F_SR_E][i] = e;
+            SRPrim q;
+            if(!sr_c2p(S, e, s.f[SPHGPU_F_SR_N][i], q)) {
+                sr_failed = true;
+                continue;
+            }
+            sr_store(i, q);
         }
     }
 
@@ -1033,8 +1473,10 @@ struct Oracle {
     {
         timestep();
         predict();
+        if(sr_failed) return err = "Lorentz factor solver did not converge", false;
         if(!make_tree() || !pre_interaction() || !fluid_force() || !gravity(exhaustive)) return false;
         correct();
+        if(sr_failed) return err = "Lorentz factor solver did not converge", false;
         time += dt;
         return true;
     }
@@ -1175,12 +1617,12 @@ int oracle_timestep(void* h)
 int oracle_predict(void* h)
 {
     static_cast<Oracle*>(h)->predict();
-    return 0;
+    return static_cast<Oracle*>(h)->sr_failed ? -1 : 0;
 }
 int oracle_correct(void* h)
 {
     static_cast<Oracle*>(h)->correct();
-    return 0;
+    return static_cast<Oracle*>(h)->sr_failed ? -1 : 0;
 }
 int oracle_initialize(void* h) { return static_cast<Oracle*>(h)->initialize() ? 0 : -1; }
 int oracle_integrate(void* h) { return static_cast<Oracle*>(h)->integrate() ? 0 : -1; }

@@ -98,6 +98,12 @@ void set_dev_params(sphgpu_ctx* c)
     d.gamma = p.gamma;
     d.cfl_sound = p.cfl_sound;
     d.cfl_force = p.cfl_force;
+    d.sr_2nd = p.sr_2nd_order;
+    d.sr_c = p.sr_c_speed;
+    d.sr_c_shock = p.sr_c_shock;
+    d.sr_c_cd = p.sr_c_cd;
+    d.sr_eta = p.sr_eta;
+    d.sr_c_smooth = p.sr_c_smooth;
     d.av_alpha = p.av_alpha;
     d.balsara = p.use_balsara_switch;
     d.td_av = p.use_time_dependent_av;
@@ -154,6 +160,8 @@ int alloc_state(sphgpu_ctx* c, DevState& s, int n)
        || (rc = dalloc(c, s.velp, n)) || (rc = dalloc(c, s.thermo, n)) || (rc = dalloc(c, s.visc, n))
        || (rc = dalloc(c, s.grad, 4 * (size_t)n)) || (rc = dalloc(c, s.id, n)) || (rc = dalloc(c, s.nbr, n)))
         return rc;
+    s.sr = nullptr;
+    if(c->prm.sph_type == SPHGPU_SRGSPH && (rc = dalloc(c, s.sr, 4 * (size_t)n))) return rc;
     return SPHGPU_OK;
 }
 
@@ -229,6 +237,12 @@ FieldRef field_ref(const DevState& s, int f)
     case SPHGPU_F_GRADH: return {s.visc, 2};
     case SPHGPU_F_PHI: return {s.visc, 3};
     case SPHGPU_F_NEIGHBOR: return {nullptr, 4};
+    case SPHGPU_F_SR_S_X: case SPHGPU_F_SR_S_Y: case SPHGPU_F_SR_S_Z: case SPHGPU_F_SR_E:
+        return {s.sr, f - SPHGPU_F_SR_S_X};
+    case SPHGPU_F_SR_N: case SPHGPU_F_SR_NU: case SPHGPU_F_SR_GAMMA_LOR: case SPHGPU_F_SR_ENTHALPY:
+        return {s.sr ? s.sr + n : nullptr, f - SPHGPU_F_SR_N};
+    case SPHGPU_F_SR_DS_X: case SPHGPU_F_SR_DS_Y: case SPHGPU_F_SR_DS_Z: case SPHGPU_F_SR_DE:
+        return {s.sr ? s.sr + 2 * n : nullptr, f - SPHGPU_F_SR_DS_X};
     default: {
         const int g = f - SPHGPU_F_GRAD_D_X;
         return {s.grad + (size_t)(g / 4) * n, g % 4};
@@ -291,8 +305,12 @@ __global__ void k_iota(int* __restrict__ id, int n)
 
 int check_params(const sphgpu_params* p, std::string& why)
 {
-    if(p->sph_type < SPHGPU_SSPH || p->sph_type > SPHGPU_GDISPH)
-        return why = "SPH type must be ssph, disph, gsph or gdisph", -1;
+    if(p->sph_type < SPHGPU_SSPH || p->sph_type > SPHGPU_SRGSPH)
+        return why = "SPH type must be ssph, disph, gsph, gdisph or srgsph", -1;
+    if(p->sph_type == SPHGPU_SRGSPH && p->precision != SPHGPU_FP64)
+        return why = "srgsph runs in the FP64 form only", -1;
+    if(p->sph_type == SPHGPU_SRGSPH && !(p->sr_c_speed > 0.0 && p->sr_eta > 0.0 && p->sr_c_smooth > 0.0))
+        return why = "srgsph needs cSpeed, etaSmoothingLength and cSmoothGradient > 0", -1;
     if(p->kernel != SPHGPU_CUBIC_SPLINE && p->kernel != SPHGPU_WENDLAND) return why = "kernel is unknown.", -1;
     if(p->neighbor_number <= 0) return why = "neighborNumber must be positive", -1;
     if(p->max_tree_level < 1 || p->max_tree_level > 21) return why = "maxTreeLevel must be in 1..21", -1;
@@ -343,6 +361,12 @@ void sphgpu_default_params(sphgpu_params* p)
     p->precision = SPHGPU_FP64;
     p->riemann_guess = SPHGPU_GUESS_NONE;
     p->mlp_max_newton = 4;
+    p->sr_2nd_order = 1;
+    p->sr_c_speed = 1.0;
+    p->sr_c_shock = 3.0;
+    p->sr_c_cd = 1.0;
+    p->sr_eta = 1.0;
+    p->sr_c_smooth = 2.0;
 }
 
 int sphgpu_device_ok(void)
@@ -415,7 +439,7 @@ int sphgpu_upload(sphgpu_ctx* c, int64_t n, const double* const* fields)
         if(src) SPHGPU_CUDA(c, cudaMemcpyAsync(stage, src, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
         const FieldRef r = field_ref(c->s, f);
         if(r.comp == 4) k_put_nbr<<<g, 256, 0, c->stream>>>(c->s.nbr, src ? stage : nullptr, (int)n);
-        else k_put<<<g, 256, 0, c->stream>>>(r.arr, r.comp, src ? stage : nullptr, (int)n);
+        else if(r.arr) k_put<<<g, 256, 0, c->stream>>>(r.arr, r.comp, src ? stage : nullptr, (int)n);
     }
     k_iota<<<g, 256, 0, c->stream>>>(c->s.id, (int)n);
     SPHGPU_CUDA(c, cudaFreeAsync(stage, c->stream));
@@ -438,6 +462,10 @@ int sphgpu_download(sphgpu_ctx* c, double* const* fields)
     for(int f = 0; f < SPHGPU_NFIELDS; ++f) {
         if(!fields[f]) continue;
         const FieldRef r = field_ref(c->s, f);
+        if(r.comp != 4 && !r.arr) {  // srgsph fields of another SPH type: zeros
+            std::fill(fields[f], fields[f] + n, 0.0);
+            continue;
+        }
         if(r.comp == 4) k_get_nbr<<<g, 256, 0, c->stream>>>(c->s.nbr, c->s.id, stage, n);
         else k_get<<<g, 256, 0, c->stream>>>(r.arr, r.comp, c->s.id, stage, n);
         SPHGPU_CUDA(c, cudaMemcpyAsync(fields[f], stage, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream));

@@ -13,6 +13,8 @@
 //          v_y (3), v_z (3) packed in that order (15 used slots)
 //   id     int32  caller index of the particle (the reference's vector index)
 //   nbr    int32  neighbour count of the last PreInteraction
+//   sr     srgsph only, 4 x n double4: {S, e}, {N, nu, gamma_lor, enthalpy},
+//          {dS/dt, de/dt}, {N before the current pre-interaction}
 // Octree nodes are stored in depth-first preorder (children in index order
 // 0..7, the order of BHNode::childs, include/bhtree.hpp:19-31) so a walk is a
 // forward scan with `skip` pointers over whole subtrees.
@@ -42,6 +44,8 @@ struct DevParams {
     double G, theta, theta2;
     int gsph2, riemann, precision, guess, mlp_max_newton;
     double ratio;  // kernel ratio 1.2 (iterative sml) or 1.0 (src/pre_interaction.cpp:31-35)
+    int sr_2nd;    // srgsph: MUSCL reconstruction
+    double sr_c, sr_c_shock, sr_c_cd, sr_eta, sr_c_smooth;
 };
 
 struct DevState {
@@ -55,6 +59,9 @@ struct DevState {
     double4* grad;  // 4 * n
     int* id;
     int* nbr;
+    // srgsph only (null otherwise), 4 * n: {S x, y, z, e}, {N, nu, gamma_lor,
+    // enthalpy}, {dS/dt x, y, z, de/dt}, {N before the current pre-interaction, -, -, -}
+    double4* sr;
 };
 
 struct DevTree {
@@ -86,6 +93,7 @@ struct DevStatus {
     unsigned long long walk_group_warps;   // warps that took the group walk
     unsigned long long walk_split_warps;   // warps walked as several sub-groups
     unsigned long long mlp_guesses;        // pairs sent to the learned guess
+    int sr_recovery;                       // srgsph: a Lorentz-factor solve did not converge
 };
 
 // Read-only 32-byte load through the non-coherent path (two 16-byte halves).

@@ -135,6 +135,12 @@ int gravity(sphgpu_ctx* c, bool direct);
 // Mixed-precision Barnes-Hut walk: FP32 node records of the current tree,
 // then the walk (one launch each).
 int gravity_nodes_mixed(sphgpu_ctx* c);
+// SRGSPH modules (srgsph.cu), dispatched from the generic ones.
+int sr_pre_interaction(sphgpu_ctx* c);
+int sr_fluid_force(sphgpu_ctx* c);
+int sr_timestep(sphgpu_ctx* c);
+int sr_predict(sphgpu_ctx* c);
+int sr_correct(sphgpu_ctx* c);
 int gravity_walk_mixed(sphgpu_ctx* c);
 int timestep(sphgpu_ctx* c);
 int predict(sphgpu_ctx* c);

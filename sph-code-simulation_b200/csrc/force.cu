@@ -613,6 +613,7 @@ __global__ void k_defer_ranges(const uint64_t* __restrict__ skeys, int n, uint64
 int fluid_force(sphgpu_ctx* c)
 {
     if(!c->have_tree) return fail(c, SPHGPU_ERR_STATE, "FluidForce before tree make");
+    if(c->prm.sph_type == SPHGPU_SRGSPH) return sr_fluid_force(c);
     const bool learned = c->prm.riemann_guess == SPHGPU_GUESS_MLP && c->prm.sph_type == SPHGPU_GSPH &&
                          c->prm.riemann_solver == SPHGPU_RIEMANN_ITERATIVE;
     if(learned && !c->have_mlp) return fail(c, SPHGPU_ERR_NO_MLP, "learned Riemann guess requested without MLP weights");

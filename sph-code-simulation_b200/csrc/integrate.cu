@@ -144,6 +144,7 @@ __global__ void k_energy_final(const double* __restrict__ part, int nb, double* 
 
 int timestep(sphgpu_ctx* c)
 {
+    if(c->prm.sph_type == SPHGPU_SRGSPH) return sr_timestep(c);
     stage_begin(c, SPHGPU_T_TIMESTEP);
     const double big = DBL_MAX;
     SPHGPU_CUDA(c, cudaMemcpyAsync(c->d_red, &big, sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -157,6 +158,7 @@ int timestep(sphgpu_ctx* c)
 
 int predict(sphgpu_ctx* c)
 {
+    if(c->prm.sph_type == SPHGPU_SRGSPH) return sr_predict(c);
     stage_begin(c, SPHGPU_T_PREDICT);
     k_predict<<<grid_for(c->n, IBLK), IBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_dt);
     SPHGPU_LAUNCH_CHECK(c, "predict");
@@ -167,6 +169,7 @@ int predict(sphgpu_ctx* c)
 
 int correct(sphgpu_ctx* c)
 {
+    if(c->prm.sph_type == SPHGPU_SRGSPH) return sr_correct(c);
     stage_begin(c, SPHGPU_T_CORRECT);
     k_correct<<<grid_for(c->n, IBLK), IBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_dt);
     SPHGPU_LAUNCH_CHECK(c, "correct");

@@ -402,6 +402,7 @@ void launch_pre(sphgpu_ctx* c)
 int pre_interaction(sphgpu_ctx* c)
 {
     if(!c->have_tree) return fail(c, SPHGPU_ERR_STATE, "PreInteraction before tree make");
+    if(c->prm.sph_type == SPHGPU_SRGSPH) return sr_pre_interaction(c);
     int rc_walk = SPHGPU_OK;
     const bool mixed = c->prm.precision == SPHGPU_MIXED;
     if(c->first_pre) {

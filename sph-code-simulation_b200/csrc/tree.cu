@@ -363,6 +363,9 @@ __global__ void k_permute(int n, const uint32_t* __restrict__ src, DevState a, D
     if(with_grad) {
         for(int g = 0; g < 4; ++g) b.grad[(size_t)g * n + p] = a.grad[(size_t)g * n + q];
     }
+    if(a.sr) {
+        for(int g = 0; g < 4; ++g) b.sr[(size_t)g * n + p] = a.sr[(size_t)g * n + q];
+    }
 }
 
 // Bottom-up mass / centre of mass (src/bhtree.cpp:154-204, 206-247).
@@ -507,7 +510,8 @@ int tree_make(sphgpu_ctx* c)
     c->node_count = nnodes;
     // leaf order + permutation of the particle state
     k_leaf_order<<<grid_for(n, BLK), BLK, 0, st>>>(n, c->d_leaf_of_start, c->t.link, c->s.id, c->d_vals);
-    k_permute<<<grid_for(n, BLK), BLK, 0, st>>>(n, c->d_vals, c->s, c->alt, c->prm.sph_type == SPHGPU_GSPH || c->prm.sph_type == SPHGPU_GDISPH,
+    k_permute<<<grid_for(n, BLK), BLK, 0, st>>>(n, c->d_vals, c->s, c->alt, c->prm.sph_type == SPHGPU_GSPH || c->prm.sph_type == SPHGPU_GDISPH ||
+                                                    c->prm.sph_type == SPHGPU_SRGSPH,
                                                 c->d_inv);
     std::swap(c->s, c->alt);
     // mass and centre of mass

@@ -15,6 +15,14 @@
 //                              extruded to 3-D with equal-mass lattices.
 //   sphgpu_sample_shock_tube   3-D shock tube along x in [-0.5,0.5] x [0,Ly]^2,
 //                              uniform lattice, left/right pressure states.
+//   sphgpu_sample_sr_shock_tube  special-relativistic Sod tube of
+//                              Solver::make_sr_sod (src/sample/sr_sod.cpp:15-
+//                              199; Kitajima et al. 2025, sec. 3.1.1) in 3-D:
+//                              left n = 1, P = 1 on a lattice of spacing dx,
+//                              right n = 0.125, P = 0.1 on spacing 2 dx, so
+//                              every particle carries the same baryon number
+//                              nu = dx^3; v = 0, conserved S = 0 and
+//                              e = gamma_lor H - P / (N c^2).
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -147,6 +155,47 @@ int64_t sphgpu_sample_shock_tube(double dx, double ly, double p_left, double p_r
         }
     }
     return n;
+}
+
+// Special-relativistic Sod tube, x in [-0.5, 0.5], y, z in [0, ly]; ly / (2 dx)
+// must be a whole number for the right lattice to tile the box.
+int64_t sphgpu_sample_sr_shock_tube(double dx, double ly, double gamma, double c_speed, double* const* f)
+{
+    const int nxl = (int)std::lround(0.5 / dx), nyl = (int)std::lround(ly / dx);
+    const int nxr = nxl / 2, nyr = nyl / 2;
+    const int64_t nl = (int64_t)nxl * nyl * nyl, nr = (int64_t)nxr * nyr * nyr;
+    if(!f) return nl + nr;
+    const double c2 = c_speed * c_speed;
+    int64_t i = 0;
+    for(int side = 0; side < 2; ++side) {
+        const int nx = side ? nxr : nxl, ny = side ? nyr : nyl;
+        const double hx = 0.5 / nx, hy = ly / ny;
+        const double n = side ? 0.125 : 1.0, P = side ? 0.1 : 1.0;
+        // one baryon number for both sides: nu = n x (volume per particle)
+        const double nu = 1.0 * (0.5 / nxl) * (ly / nyl) * (ly / nyl);
+        const double u = P / ((gamma - 1.0) * n);
+        const double H = 1.0 + u / c2 + P / (n * c2);
+        const double N = 1.0 * n;
+        const double e = 1.0 * H - P / (N * c2);
+        for(int a = 0; a < nx; ++a) {
+            for(int b = 0; b < ny; ++b) {
+                for(int c = 0; c < ny; ++c, ++i) {
+                    put(f, SPHGPU_F_POS_X, i, (side ? 0.0 : -0.5) + (a + 0.5) * hx);
+                    put(f, SPHGPU_F_POS_Y, i, (b + 0.5) * hy);
+                    put(f, SPHGPU_F_POS_Z, i, (c + 0.5) * hy);
+                    put(f, SPHGPU_F_MASS, i, nu);
+                    put(f, SPHGPU_F_DENS, i, n);
+                    put(f, SPHGPU_F_PRES, i, P);
+                    put(f, SPHGPU_F_ENE, i, u);
+                    put(f, SPHGPU_F_SR_E, i, e);
+                    put(f, SPHGPU_F_SR_N, i, N);
+                    put(f, SPHGPU_F_SR_NU, i, nu);
+                    put(f, SPHGPU_F_SR_GAMMA_LOR, i, 1.0);
+                }
+            }
+        }
+    }
+    return nl + nr;
 }
 
 }  // extern "C"

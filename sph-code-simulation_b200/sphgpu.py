@@ -25,7 +25,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsphgpu.so")
 
 # enums (include/sphgpu.h)
-SSPH, DISPH, GSPH, GDISPH = 0, 1, 2, 3
+SSPH, DISPH, GSPH, GDISPH, SRGSPH = 0, 1, 2, 3, 4
 CUBIC_SPLINE, WENDLAND = 0, 1
 RIEMANN_HLL, RIEMANN_ITERATIVE = 0, 1
 FP64, MIXED = 0, 1
@@ -38,6 +38,8 @@ FIELDS = [
     "grad_d_x", "grad_d_y", "grad_d_z", "grad_p_x", "grad_p_y", "grad_p_z",
     "grad_v0_x", "grad_v0_y", "grad_v0_z", "grad_v1_x", "grad_v1_y", "grad_v1_z",
     "grad_v2_x", "grad_v2_y", "grad_v2_z",
+    "sr_S_x", "sr_S_y", "sr_S_z", "sr_e", "sr_N", "sr_nu", "sr_gamma_lor", "sr_enthalpy",
+    "sr_dS_x", "sr_dS_y", "sr_dS_z", "sr_de",
 ]
 NFIELDS = len(FIELDS)
 FIELD_INDEX = {f: k for k, f in enumerate(FIELDS)}
@@ -62,7 +64,8 @@ class Params(C.Structure):
         ("range_min", C.c_double * 3), ("range_max", C.c_double * 3), ("use_gravity", C.c_int32),
         ("gsph_2nd_order", C.c_int32), ("g_constant", C.c_double), ("theta", C.c_double),
         ("riemann_solver", C.c_int32), ("precision", C.c_int32), ("riemann_guess", C.c_int32),
-        ("mlp_max_newton", C.c_int32),
+        ("mlp_max_newton", C.c_int32), ("sr_2nd_order", C.c_int32), ("sr_c_speed", C.c_double),
+        ("sr_c_shock", C.c_double), ("sr_c_cd", C.c_double), ("sr_eta", C.c_double), ("sr_c_smooth", C.c_double),
     ]
 
     def copy(self) -> "Params":
@@ -266,6 +269,13 @@ def sample_shock_tube(dx: float, ly: float = 0.05, p_left: float = 1000.0, p_rig
     """3-D shock tube along x in [-0.5, 0.5] x [0, ly]^2."""
     return _sample(lib().sphgpu_sample_shock_tube, C.c_double(dx), C.c_double(ly), C.c_double(p_left),
                    C.c_double(p_right), C.c_double(gamma))
+
+
+def sample_sr_shock_tube(dx: float, ly: float = 0.05, gamma: float = 5.0 / 3.0,
+                         c_speed: float = 1.0) -> Dict[str, np.ndarray]:
+    """Special-relativistic Sod tube in 3-D (left n = 1, P = 1; right n = 0.125, P = 0.1)."""
+    return _sample(lib().sphgpu_sample_sr_shock_tube, C.c_double(dx), C.c_double(ly), C.c_double(gamma),
+                   C.c_double(c_speed))
 
 
 class Simulation:
@@ -534,6 +544,10 @@ def config_params(name: str, **overrides) -> Params:
                            riemann_solver=RIEMANN_HLL, gamma=1.4, periodic=1, use_balsara_switch=1,
                            use_time_dependent_av=1, alpha_min=0.1, alpha_max=2.0, epsilon_av=0.2, av_alpha=1.0,
                            use_ac=1, alpha_ac=1.0, range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.05, 0.05))
+    elif name == "tube_srgsph":        # special-relativistic gsph Sod tube, MUSCL, exact SR solver, cubic, K=50
+        p = default_params(sph_type=SRGSPH, kernel=CUBIC_SPLINE, neighbor_number=50, sr_2nd_order=1,
+                           gamma=5.0 / 3.0, periodic=1, range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.05, 0.05),
+                           sr_c_speed=1.0, sr_c_shock=3.0, sr_c_cd=1.0, sr_eta=1.0, sr_c_smooth=2.0)
     elif name == "evrard_disph":       # disph + gravity sphere, Wendland, K=128, TD-AV, AC
         p = default_params(sph_type=DISPH, kernel=WENDLAND, neighbor_number=128, use_time_dependent_av=1,
                            alpha_min=0.1, alpha_max=2.0, epsilon_av=0.2, use_balsara_switch=1, use_ac=1,

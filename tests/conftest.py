@@ -45,9 +45,12 @@ def golden(name):
 
 
 def params_from_bytes(G, raw):
+    """Parameters stored as raw struct bytes; fields appended to the struct
+    after the fixture was written keep their defaults."""
     import ctypes
-    p = G.Params()
-    ctypes.memmove(ctypes.byref(p), bytes(raw.tobytes()), ctypes.sizeof(p))
+    p = G.default_params()
+    b = bytes(raw.tobytes())
+    ctypes.memmove(ctypes.byref(p), b, min(len(b), ctypes.sizeof(p)))
     return p
 
 

@@ -31,6 +31,13 @@ oracle/_ref/libsphref*.so, driven by oracle/ref_harness.cpp):
                      K = 0.5), with the reference's table
                      data/lane_emden/n1.5_3d.dat (xi, theta, dtheta, xi_1):
                      states after each step and dt_relax.
+  sr_tube.npz        SRGSPH (src/srgsph/*.cpp) on a 3-D special-relativistic
+                     Sod tube: states after Solver::initialize, after one
+                     predict and one correct with a small fixed dt, and the
+                     error a full integrate step stops with (the reference's
+                     exact SR Riemann solver returns spurious star pressures
+                     for nearly equal states, and the primitive recovery then
+                     fails), for first / second order and fixed / iterative h.
   lists_<cfg>.npz    Distance-sorted neighbour lists (CSR) from
                      BHTree::neighbor_search and from exhaustive_search
                      (gather and is_ij) at the state after initialize.
@@ -211,6 +218,90 @@ def relax_golden(steps=3, alpha=0.3, K=0.5):
     print("relax_evrard: dt_relax", dts)
 
 
+SR_FIELDS = ["pos_x", "pos_y", "pos_z", "vel_x", "vel_y", "vel_z", "velp_x", "velp_y", "velp_z", "dens", "pres",
+             "ene", "ene_p", "sml", "sound", "grad_d_x", "grad_d_y", "grad_d_z", "grad_p_x", "grad_p_y", "grad_p_z",
+             "grad_v0_x", "grad_v0_y", "grad_v0_z", "grad_v1_x", "grad_v1_y", "grad_v1_z", "grad_v2_x", "grad_v2_y",
+             "grad_v2_z", "sr_S_x", "sr_S_y", "sr_S_z", "sr_e", "sr_N", "sr_nu", "sr_gamma_lor", "sr_enthalpy",
+             "sr_dS_x", "sr_dS_y", "sr_dS_z", "sr_de"]
+
+
+def sr_golden():
+    """SRGSPH on a 3-D special-relativistic Sod tube (dx = 0.025, 360 particles,
+    eta = 2.3, first / second order, fixed / iterative smoothing length): the
+    state after Solver::initialize, after Solver::predict and Solver::correct
+    with a dt of 1e-6 e_min / max|rate| (so every primitive recovery
+    converges), and the error a full Solver::integrate stops with."""
+    out = {}
+    for order in (0, 1):
+        for it in (0, 1):
+            tag = f"o{order}i{it}"
+            p = G.config_params("tube_srgsph", sr_2nd_order=order, iterative_sml=it, sr_eta=2.3,
+                                range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.1, 0.1))
+            fields = G.sample_sr_shock_tube(0.025, ly=0.1)
+            ref = O.Reference(p, fields)
+            ref.initialize()
+            s0 = ref.download(SR_FIELDS)
+            big = max(np.abs(s0[k]).max() for k in ("sr_dS_x", "sr_dS_y", "sr_dS_z", "sr_de"))
+            dt = 1e-6 * s0["sr_e"].min() / big
+            ref.set_dt(dt)
+            ref.predict()
+            s1 = ref.download(SR_FIELDS)
+            ref.correct()
+            s2 = ref.download(SR_FIELDS)
+            ref2 = O.Reference(p, fields)
+            ref2.initialize()
+            try:
+                ref2.integrate()
+                msg = ""
+            except RuntimeError as e:
+                msg = str(e).split("failed: ", 1)[-1]
+            out[tag + "_params"] = np.frombuffer(bytes(p), dtype=np.uint8)
+            out[tag + "_dt"] = dt
+            out[tag + "_integrate_error"] = msg
+            for k, st in enumerate((s0, s1, s2)):
+                for f, v in st.items():
+                    out[f"{tag}_s{k}_{f}"] = v
+            print(f"sr_tube {tag}: dt_check {dt:.3e}; integrate: {msg or 'ok'}")
+    fields = G.sample_sr_shock_tube(0.025, ly=0.1)
+    for f in ("pos_x", "pos_y", "pos_z", "mass", "dens", "pres", "ene", "sr_e", "sr_N", "sr_nu", "sr_gamma_lor"):
+        out["ic_" + f] = fields[f]
+    # FluidForce alone on a prescribed two-state tube, where every Riemann
+    # problem is well posed: equal states inside each half (exact star state
+    # at the first iterate) and a Sod-size jump across the interface (n 1 /
+    # 0.125, P 1 / 0.08, so |log10 P_i/P_j| > cContactDiscontinuity and the
+    # second-order path falls back to first order there as well)
+    st = sr_force_state(fields)
+    for order in (0, 1):
+        p = G.config_params("tube_srgsph", sr_2nd_order=order, sr_eta=2.3, range_min=(-0.5, 0.0, 0.0),
+                            range_max=(0.5, 0.1, 0.1))
+        ref = O.Reference(p, st)
+        ref.tree_make()
+        ref.set_kernel()
+        ref.fluid_force()
+        r = ref.download(["sr_dS_x", "sr_dS_y", "sr_dS_z", "sr_de"])
+        out[f"force_o{order}_params"] = np.frombuffer(bytes(p), dtype=np.uint8)
+        for k, v in r.items():
+            out[f"force_o{order}_{k}"] = v
+        print(f"sr_tube force o{order}: max |dS_x| {np.abs(r['sr_dS_x']).max():.3e}")
+    for k, v in st.items():
+        out["fst_" + k] = v
+    np.savez_compressed(os.path.join(OUT, "sr_tube.npz"), **out)
+
+
+def sr_force_state(fields, gamma=5.0 / 3.0):
+    """Primitive state of the two-state SR tube as the force reads it."""
+    left = fields["pos_x"] < 0.0
+    n = np.where(left, 1.0, 0.125)
+    P = np.where(left, 1.0, 0.08)
+    H = 1.0 + gamma * P / ((gamma - 1.0) * n)
+    nu = fields["sr_nu"]
+    st = {k: fields[k].copy() for k in ("pos_x", "pos_y", "pos_z", "mass", "sr_nu")}
+    st.update({"dens": n, "pres": P, "sr_N": n.copy(), "sr_gamma_lor": np.ones_like(n), "sr_enthalpy": H,
+               "sound": np.sqrt((gamma - 1.0) * (H - 1.0) / H), "ene": P / ((gamma - 1.0) * n),
+               "sml": 2.3 * np.cbrt(nu / n)})
+    return st
+
+
 def main():
     O.build(reference=True)
     if not O.have_reference():
@@ -222,6 +313,7 @@ def main():
         lists(name)
     csv_golden()
     relax_golden()
+    sr_golden()
 
 
 if __name__ == "__main__":

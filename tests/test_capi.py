@@ -38,7 +38,8 @@ def test_default_params_match_reference_defaults(G):
 def test_params_struct_layout(G):
     import ctypes
     # offsets of the C struct (natural alignment), checked against ctypes
-    assert ctypes.sizeof(G.Params) == 192
+    assert ctypes.sizeof(G.Params) == 240
+    assert G.Params.sr_2nd_order.offset == 192 and G.Params.sr_c_speed.offset == 200
 
 
 def test_samples(G):
@@ -50,6 +51,11 @@ def test_samples(G):
     assert np.all((sh["pos_y"] > 0.25) & (sh["pos_y"] < 0.75) == (sh["dens"] == 2.0))
     tu = G.sample_shock_tube(0.025, ly=0.1)
     assert np.all((tu["pos_x"] < 0) == (tu["pres"] == 1000.0))
+    sr = G.sample_sr_shock_tube(0.025, ly=0.1)
+    left = sr["pos_x"] < 0
+    assert left.sum() == 320 and (~left).sum() == 40
+    assert np.all(sr["sr_nu"] == sr["sr_nu"][0]) and np.all(sr["sr_S_x"] == 0.0)
+    assert np.all(sr["sr_N"][left] == 1.0) and np.all(sr["sr_N"][~left] == 0.125)
 
 
 def test_create_without_device_fails_loudly(G):
