@@ -45,7 +45,7 @@ extern "C" {
 /* ---- enums: same order as sph::SPHType / KernelType / RiemannSolverType
  *      (include/parameters.hpp:8-31) ---- */
 enum sphgpu_sph_type { SPHGPU_SSPH = 0, SPHGPU_DISPH = 1, SPHGPU_GSPH = 2, SPHGPU_GDISPH = 3, SPHGPU_SRGSPH = 4 };
-enum sphgpu_kernel   { SPHGPU_CUBIC_SPLINE = 0, SPHGPU_WENDLAND = 1 };
+enum sphgpu_kernel   { SPHGPU_CUBIC_SPLINE = 0, SPHGPU_WENDLAND = 1, SPHGPU_GAUSSIAN = 2 };
 enum sphgpu_riemann  { SPHGPU_RIEMANN_HLL = 0, SPHGPU_RIEMANN_ITERATIVE = 1 };
 enum sphgpu_precision { SPHGPU_FP64 = 0, SPHGPU_MIXED = 1 };
 enum sphgpu_guess    { SPHGPU_GUESS_NONE = 0, SPHGPU_GUESS_MLP = 1 };

@@ -86,7 +86,8 @@ std::shared_ptr<SPHParameters> to_param(const sphgpu_params* p)
     q->tree.leaf_particle_num = p->leaf_particle_num;
     q->physics.neighbor_number = p->neighbor_number;
     q->physics.gamma = p->gamma;
-    q->kernel = p->kernel == SPHGPU_WENDLAND ? KernelType::WENDLAND : KernelType::CUBIC_SPLINE;
+    q->kernel = p->kernel == SPHGPU_WENDLAND ? KernelType::WENDLAND
+              : p->kernel == SPHGPU_GAUSSIAN ? KernelType::GAUSSIAN : KernelType::CUBIC_SPLINE;
     q->iterative_sml = p->iterative_sml != 0;
     q->periodic.is_valid = p->periodic != 0;
     for(int k = 0; k < DIM; ++k) {

@@ -107,12 +107,48 @@ struct WendlandC4 {
     }
 };
 
+// include/kernel/gaussian_kernel.hpp:21-57 (DIM = 3): W = sigma / h^3 exp(-q^2),
+// sigma = 1 / pi^(3/2) written to 15 digits as the reference writes it.
+struct Gauss {
+    static constexpr real sigma = 0.179587122125167;
+    static real w(real r, real h)
+    {
+        const real q = r / h;
+        const real q2 = q * q;
+        return sigma / pow3(h) * std::exp(-q2);
+    }
+    static real dw(real r, real h)
+    {
+        if(r == 0.0) return 0.0;
+        const real q = r / h;
+        const real q2 = q * q;
+        const real wv = sigma / pow3(h) * std::exp(-q2);
+        return -2.0 * wv * q / (h * r);
+    }
+    static real dhw(real r, real h)
+    {
+        const real q = r / h;
+        const real q2 = q * q;
+        const real wv = sigma / pow3(h) * std::exp(-q2);
+        return wv * (2.0 * q2 - static_cast<real>(3)) / h;
+    }
+};
+
 struct Kernel {
     int type;
-    real w(real r, real h) const { return type == SPHGPU_WENDLAND ? WendlandC4::w(r, h) : CubicSpline::w(r, h); }
-    real dwc(real r, real h) const { return type == SPHGPU_WENDLAND ? WendlandC4::dw(r, h) : CubicSpline::dw(r, h); }
+    real w(real r, real h) const
+    {
+        return type == SPHGPU_WENDLAND ? WendlandC4::w(r, h) : type == SPHGPU_GAUSSIAN ? Gauss::w(r, h) : CubicSpline::w(r, h);
+    }
+    real dwc(real r, real h) const
+    {
+        return type == SPHGPU_WENDLAND ? WendlandC4::dw(r, h) : type == SPHGPU_GAUSSIAN ? Gauss::dw(r, h) : CubicSpline::dw(r, h);
+    }
     V3 dw(V3 rij, real r, real h) const { return rij * dwc(r, h); }
-    real dhw(real r, real h) const { return type == SPHGPU_WENDLAND ? WendlandC4::dhw(r, h) : CubicSpline::dhw(r, h); }
+    real dhw(real r, real h) const
+    {
+        return type == SPHGPU_WENDLAND ? WendlandC4::dhw(r, h) : type == SPHGPU_GAUSSIAN ? Gauss::dhw(r, h) : CubicSpline::dhw(r, h);
+    }
 };
 
 // ---------------------------------------------------------------- periodic

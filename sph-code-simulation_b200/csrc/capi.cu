@@ -311,7 +311,8 @@ int check_params(const sphgpu_params* p, std::string& why)
         return why = "srgsph runs in the FP64 form only", -1;
     if(p->sph_type == SPHGPU_SRGSPH && !(p->sr_c_speed > 0.0 && p->sr_eta > 0.0 && p->sr_c_smooth > 0.0))
         return why = "srgsph needs cSpeed, etaSmoothingLength and cSmoothGradient > 0", -1;
-    if(p->kernel != SPHGPU_CUBIC_SPLINE && p->kernel != SPHGPU_WENDLAND) return why = "kernel is unknown.", -1;
+    if(p->kernel != SPHGPU_CUBIC_SPLINE && p->kernel != SPHGPU_WENDLAND && p->kernel != SPHGPU_GAUSSIAN)
+        return why = "kernel is unknown.", -1;
     if(p->neighbor_number <= 0) return why = "neighborNumber must be positive", -1;
     if(p->max_tree_level < 1 || p->max_tree_level > 21) return why = "maxTreeLevel must be in 1..21", -1;
     if(p->leaf_particle_num < 1) return why = "leafParticleNumber must be >= 1", -1;

@@ -152,9 +152,13 @@ __device__ __forceinline__ double abs2x(Vec3d d)
 
 // ------------------------------------------------------------ SPH kernels
 // W, grad W (as the scalar c with grad W = r_ij c) and dW/dh for the cubic
-// spline (include/kernel/cubic_spline.hpp:21-53) and Wendland C4
-// (include/kernel/wendland_kernel.hpp:23-49), DIM = 3, restated from the
+// spline (include/kernel/cubic_spline.hpp:21-53), Wendland C4
+// (include/kernel/wendland_kernel.hpp:23-49) and the Gaussian
+// W = exp(-(r/h)^2) / (h^3 pi^(3/2)) that the reference cuts at r = h like the
+// others (include/kernel/gaussian_kernel.hpp:21-57), DIM = 3, restated from the
 // formulas; T = double (plain form) or float (mixed form).
+// 1 / pi^(3/2) as the reference writes it (to 15 digits)
+constexpr double GAUSS_SIGMA = 0.179587122125167;
 template <typename T>
 struct Kern {
     static constexpr double PI = 3.14159265358979323846;
@@ -164,6 +168,10 @@ struct Kern {
 
     __device__ static __forceinline__ T w(int type, T r, T h)
     {
+        if(type == SPHGPU_GAUSSIAN) {
+            const T q = r / h;
+            return T(GAUSS_SIGMA) / cube(h) * exp(-(q * q));
+        }
         if(type == SPHGPU_WENDLAND) {
             const T sigma = T(495.0 / (32.0 * PI));
             const T q = r / h;
@@ -180,6 +188,12 @@ struct Kern {
 
     __device__ static __forceinline__ T dwc(int type, T r, T h)
     {
+        if(type == SPHGPU_GAUSSIAN) {
+            if(r == T(0)) return T(0);
+            const T q = r / h;
+            const T wv = T(GAUSS_SIGMA) / cube(h) * exp(-(q * q));
+            return T(-2) * wv * q / (h * r);
+        }
         if(type == SPHGPU_WENDLAND) {
             const T sigma = T(495.0 / (32.0 * PI));
             const T q = r / h;
@@ -197,6 +211,11 @@ struct Kern {
 
     __device__ static __forceinline__ T dhw(int type, T r, T h)
     {
+        if(type == SPHGPU_GAUSSIAN) {
+            const T q = r / h;
+            const T wv = T(GAUSS_SIGMA) / cube(h) * exp(-(q * q));
+            return wv * (T(2) * (q * q) - T(3)) / h;
+        }
         if(type == SPHGPU_WENDLAND) {
             const T sigma = T(495.0 / (32.0 * PI));
             const T q = r / h;
@@ -227,6 +246,13 @@ struct KernH {
     __device__ __forceinline__ KernH(int type_, T h) : type(type_)
     {
         constexpr double PI = 3.14159265358979323846;
+        if(type == SPHGPU_GAUSSIAN) {
+            inv = T(1) / h;
+            wn = T(GAUSS_SIGMA) * inv * inv * inv;
+            dwn = T(-2) * wn * inv;  // times q / r
+            dhn = wn * inv;
+            return;
+        }
         if(type == SPHGPU_WENDLAND) {
             const T sigma = T(495.0 / (32.0 * PI));
             inv = T(1) / h;
@@ -246,6 +272,7 @@ struct KernH {
     __device__ __forceinline__ T w(T r) const
     {
         const T q = r * inv;
+        if(type == SPHGPU_GAUSSIAN) return wn * exp(-(q * q));
         if(type == SPHGPU_WENDLAND) {
             const T a = T(0.5) * (T(1) - q + fabs(T(1) - q));
             const T a2 = a * a;
@@ -258,6 +285,7 @@ struct KernH {
     __device__ __forceinline__ T dwc(T r, T rinv) const
     {
         const T q = r * inv;
+        if(type == SPHGPU_GAUSSIAN) return r == T(0) ? T(0) : dwn * exp(-(q * q)) * q * rinv;
         if(type == SPHGPU_WENDLAND) {
             const T a = T(0.5) * (T(1) - q + fabs(T(1) - q));
             const T a2 = a * a;
@@ -271,6 +299,7 @@ struct KernH {
     __device__ __forceinline__ T dhw(T r) const
     {
         const T q = r * inv;
+        if(type == SPHGPU_GAUSSIAN) return dhn * exp(-(q * q)) * (T(2) * (q * q) - T(3));
         if(type == SPHGPU_WENDLAND) {
             const T a = T(0.5) * (T(1) - q + fabs(T(1) - q));
             const T a2 = a * a;

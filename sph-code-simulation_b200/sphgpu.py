@@ -26,7 +26,7 @@ LIB_PATH = os.path.join(HERE, "libsphgpu.so")
 
 # enums (include/sphgpu.h)
 SSPH, DISPH, GSPH, GDISPH, SRGSPH = 0, 1, 2, 3, 4
-CUBIC_SPLINE, WENDLAND = 0, 1
+CUBIC_SPLINE, WENDLAND, GAUSSIAN = 0, 1, 2
 RIEMANN_HLL, RIEMANN_ITERATIVE = 0, 1
 FP64, MIXED = 0, 1
 GUESS_NONE, GUESS_MLP = 0, 1

@@ -18,7 +18,8 @@ oracle/_ref/libsphref*.so, driven by oracle/ref_harness.cpp):
                      row, the recomputed full-precision values for the same
                      particles, and W0.
   steps_<cfg>.npz    Small instances of the benchmark workloads (and of the
-                     gdisph shock tube, first and second order): the
+                     gdisph shock tube, first and second order, and of the
+                     ssph Evrard sphere with the Gaussian kernel): the
                      full particle state after Solver::initialize and after
                      each of two Solver::integrate steps, plus dt.
   csv_snapshots.npz  Lines of two CSV v1 snapshots the reference ships
@@ -80,6 +81,7 @@ SMALL = {
                     lambda: G.sample_shear_layer(0.05, lz=0.125)),
     "tube_gdisph": (lambda: G.config_params("tube_gdisph", range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.1, 0.1)),
                     lambda: G.sample_shock_tube(0.025, ly=0.1)),
+    "evrard_ssph_gauss": (lambda: G.config_params("evrard_ssph", kernel=G.GAUSSIAN), lambda: G.sample_evrard(12)),
     "tube_gdisph_1st": (lambda: G.config_params("tube_gdisph", gsph_2nd_order=0, use_balsara_switch=0,
                                                 range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.1, 0.1)),
                         lambda: G.sample_shock_tube(0.025, ly=0.1)),

@@ -21,7 +21,7 @@ from conftest import golden, params_from_bytes, rel_err
 
 pytestmark = pytest.mark.gpu
 
-SMALL = ["evrard_ssph", "evrard_disph", "tube_gsph", "tube_gsph_hll", "shear_disph", "tube_gdisph",
+SMALL = ["evrard_ssph", "evrard_ssph_gauss", "evrard_disph", "tube_gsph", "tube_gsph_hll", "shear_disph", "tube_gdisph",
          "tube_gdisph_1st"]
 PRE_FIELDS = ["dens", "pres", "sml", "gradh", "balsara", "alpha"]
 

@@ -9,7 +9,7 @@ import pytest
 
 from conftest import golden, params_from_bytes
 
-SMALL = ["evrard_ssph", "evrard_disph", "tube_gsph", "tube_gsph_hll", "shear_disph", "tube_gdisph",
+SMALL = ["evrard_ssph", "evrard_ssph_gauss", "evrard_disph", "tube_gsph", "tube_gsph_hll", "shear_disph", "tube_gdisph",
          "tube_gdisph_1st"]
 
 
@@ -79,7 +79,7 @@ def test_oracle_neighbor_lists(G, O, name):
             np.testing.assert_array_equal(ids, g[f"{tag}_ij{ij}_ids"])
 
 
-@pytest.mark.parametrize("kind", [0, 1])
+@pytest.mark.parametrize("kind", [0, 1, 2])
 def test_kernel_derivatives(O, kind):
     """dW/dr and dW/dh against central differences (test/kernel_test/kernel_test.cpp:8-85)."""
     prev = None
@@ -99,11 +99,15 @@ def test_kernel_derivatives(O, kind):
 
 
 def test_kernel_normalisation(O):
-    """4 pi int_0^h W r^2 dr = 1 for both kernels."""
+    """4 pi int_0^h W r^2 dr = 1 for the compact kernels."""
     r = np.linspace(0, 1, 20001)
     for kind in (0, 1):
         w = np.array([O.kernel_w(kind, x, 1.0) for x in r])
         assert np.trapezoid(4 * np.pi * r * r * w, r) == pytest.approx(1.0, rel=1e-6)
+    # the Gaussian is normalised over all space (the neighbour search cuts it at h)
+    r = np.linspace(0, 8, 40001)
+    w = np.array([O.kernel_w(2, x, 1.0) for x in r])
+    assert np.trapezoid(4 * np.pi * r * r * w, r) == pytest.approx(1.0, rel=1e-9)
 
 
 def test_riemann_solvers(O):
