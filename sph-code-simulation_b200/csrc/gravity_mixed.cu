@@ -30,7 +30,6 @@
 #include <cuda_runtime.h>
 
 #include "context.cuh"
-#include "softening.cuh"
 
 namespace sphgpu {
 
@@ -66,6 +65,28 @@ __global__ void k_gnode(DevTree Tr, double G, GNode* __restrict__ rec, int cap)
     }
 }
 
+// Spline softening of one pair in FP32: the kernels f (potential) and g (force
+// / r) of the Hernquist & Katz spline (src/bhtree.cpp:318-345) for one smoothing length,
+// with their divisions by e = h / 2 and by r turned into products with the
+// reciprocals einv = 1 / e and rinv = 1 / r.
+__device__ __forceinline__ void hk_fg(float r, float rinv, float einv, float& f, float& g)
+{
+    const float u = r * einv;
+    const float u2 = u * u;
+    if(u < 1.f) {
+        f = (-0.5f * u2 * (1.f / 3.f - 0.15f * u2 + u2 * u * 0.05f) + 1.4f) * einv;
+        g = (4.f / 3.f - 1.2f * u2 + 0.5f * u2 * u) * (einv * einv * einv);
+    } else if(u < 2.f) {
+        const float u3 = u2 * u;
+        f = -(1.f / 15.f) * rinv + (-u2 * (4.f / 3.f - u + 0.3f * u2 - u3 * (1.f / 30.f)) + 1.6f) * einv;
+        g = (-1.f / 15.f + 8.f / 3.f * u3 - 3.f * u3 * u + 1.2f * u3 * u2 - u3 * u3 * (1.f / 6.f)) *
+            (rinv * rinv * rinv);
+    } else {
+        f = rinv;
+        g = rinv * rinv * rinv;
+    }
+}
+
 // Minimum image of an FP32 offset (include/periodic.hpp:34-72): the closest of
 // d, d + L, d - L.
 __device__ __forceinline__ float min_image_f(float d, float L)
@@ -96,7 +117,7 @@ __global__ void __launch_bounds__(MBLK, 8) k_gravity_mixed(DevParams P, DevState
     }
     const float xh = (float)xi, yh = (float)yi, zh = (float)zi;
     const float xl = (float)(xi - (double)xh), yl = (float)(yi - (double)yh), zl = (float)(zi - (double)zh);
-    const float hif = (float)hi;
+    const float einv_i = (float)(2.0 / hi);  // 1 / e, e = h / 2
     const float theta2 = (float)P.theta2;
     const float Gf = (float)P.G;
     const bool per = P.periodic;
@@ -138,13 +159,18 @@ __global__ void __launch_bounds__(MBLK, 8) k_gravity_mixed(DevParams P, DevState
             for(int q = lk.x; q < lk.y; ++q) {
                 if(q == i) continue;
                 const double4 pq = ldg4(&S.pos[q]);
-                const float hq = (float)ldg4(&S.vel[q]).w;
+                const float hq = (float)__ldg(&S.vel[q].w);
                 const Vec3d r = rij(P, xi, yi, zi, pq.x, pq.y, pq.z);
                 const float rx = (float)r.x, ry = (float)r.y, rz = (float)r.z;
-                const float rr = sqrtf(rx * rx + ry * ry + rz * rz);
+                const float r2 = rx * rx + ry * ry + rz * rz;
+                const float rinv = rsqrtf(r2);
+                const float rr = r2 * rinv;
+                float f1, g1, f2, g2;
+                hk_fg(rr, rinv, einv_i, f1, g1);
+                hk_fg(rr, rinv, __fdividef(2.f, hq), f2, g2);
                 const float gm = Gf * (float)pq.w;
-                fp -= gm * (hk_f<float>(rr, hif) + hk_f<float>(rr, hq)) * 0.5f;
-                const float c = gm * (hk_g<float>(rr, hif) + hk_g<float>(rr, hq)) * 0.5f;
+                fp -= gm * (f1 + f2) * 0.5f;
+                const float c = gm * (g1 + g2) * 0.5f;
                 fx -= rx * c;
                 fy -= ry * c;
                 fz -= rz * c;
