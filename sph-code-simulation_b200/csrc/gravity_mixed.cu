@@ -23,7 +23,11 @@
 // Measured alternatives on the same sphere: a warp-synchronous walk (cursor =
 // the warp's smallest next node, broadcast loads) 9.96 ms vs 9.30 ms per-lane
 // with three loads; walks shared by 2, 4, 8, 16 lanes 17.6 / 14.2 / 12.3 /
-// 11.3 ms; queueing opened leaves for warp-wide pair batches 9.65 ms.
+// 11.3 ms; queueing opened leaves for warp-wide pair batches 9.65 ms.  With
+// the present records and pair terms (6.31 ms): lanes that take the next
+// particle of a per-warp range when their walk ends, instead of waiting for
+// the warp's longest walk, 10.07 ms (the lanes' walks drift apart and lose
+// the L1 reuse of walking neighbouring particles in step).
 // The records are rebuilt from the tree on every call (one streaming pass over
 // the nodes), so they always match the current tree.
 #include <cuda_bf16.h>
