@@ -148,6 +148,8 @@ typedef struct sphgpu_counters {
     int64_t walk_split_warps;      /* warps walked as several sub-groups     */
     int64_t walk_fallbacks;        /* group walks redone per lane (overflow) */
     int64_t mlp_guesses;           /* pairs whose start came from the network */
+    int64_t force_list_builds;     /* FluidForce calls that took the pair lists
+                                      built from the gather lists (no walk) */
 } sphgpu_counters;
 
 /* Stage timers (ms, summed since the last reset; CUDA events on the
@@ -197,6 +199,14 @@ int sphgpu_tree_set_kernel(sphgpu_ctx* ctx);
    order (not distance-sorted). */
 int sphgpu_neighbor_search(sphgpu_ctx* ctx, int is_ij, int64_t* offsets,
                            int32_t* ids, int64_t ids_capacity);
+/* The pairs FluidForce sums over for the current state, as a CSR in caller
+   order like sphgpu_neighbor_search: every j with r_ij < max(h_i, h_j).
+   After PreInteraction they are built from the gather lists (own entries in
+   gather-list order, then the pairs only j's kernel reaches, by index);
+   otherwise, or when those are incomplete, the symmetric walk's lists.  No
+   reference counterpart (the reference searches inside FluidForce::calculation,
+   src/fluid_force.cpp:45-60); parity checks use it. */
+int sphgpu_force_pairs(sphgpu_ctx* ctx, int64_t* offsets, int32_t* ids, int64_t ids_capacity);
 /* Same, with the O(N^2) exhaustive predicate of exhaustive_search
    (src/exhaustive_search.cpp:11-42). Debug/parity only. */
 int sphgpu_exhaustive_search(sphgpu_ctx* ctx, int is_ij, int64_t* offsets,

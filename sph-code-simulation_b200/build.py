@@ -26,7 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
            "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 EXACT = {"tree.cu", "walk.cu", "gravity.cu", "integrate.cu", "noalloc.cu", "relax.cu", "srgsph.cu"}
-SOURCES = ["scan_sort.cu", "tree.cu", "walk.cu", "pre.cu", "force.cu", "gravity.cu", "gravity_mixed.cu",
+SOURCES = ["scan_sort.cu", "tree.cu", "walk.cu", "pre.cu", "force.cu", "gravity.cu", "gravity_mixed.cu", "flist.cu",
            "integrate.cu", "mlp.cu", "capi.cu", "noalloc.cu", "relax.cu", "srgsph.cu"]
 HOST_SOURCES = ["samples.cpp", "csv.cpp"]
 

@@ -408,6 +408,9 @@ int sphgpu_destroy(sphgpu_ctx* c)
     if(c->d_mlp) cudaFree(c->d_mlp);
     if(c->d_mlp_master) cudaFree(c->d_mlp_master);
     if(c->d_relax) cudaFree(c->d_relax);
+    if(c->d_tcount) cudaFree(c->d_tcount);
+    if(c->d_flist_flags) cudaFree(c->d_flist_flags);
+    if(c->d_rsearch) cudaFree(c->d_rsearch);
     if(c->d_gnode) cudaFree(c->d_gnode);
     if(c->d_mlp_defer) cudaFree(c->d_mlp_defer);
     if(c->d_harvest) cudaFree(c->d_harvest);
@@ -447,6 +450,7 @@ int sphgpu_upload(sphgpu_ctx* c, int64_t n, const double* const* fields)
     SPHGPU_LAUNCH_CHECK(c, "upload");
     SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
     c->have_tree = false;
+    c->flist_ready = false;
     c->first_pre = true;
     c->time = 0.0;
     return SPHGPU_OK;
@@ -535,6 +539,16 @@ int sphgpu_neighbor_search(sphgpu_ctx* c, int is_ij, int64_t* offsets, int32_t* 
     const int rc = is_ij ? pair_walk(c) : gather_walk(c, false, 1.0);
     if(rc < 0) return rc;
     return export_lists(c, is_ij ? 1 : 0, offsets, ids, cap);
+}
+
+int sphgpu_force_pairs(sphgpu_ctx* c, int64_t* offsets, int32_t* ids, int64_t cap)
+{
+    SPHGPU_NEED_STATE(c);
+    if(!offsets) return SPHGPU_ERR_ARG;
+    if(!c->have_tree) return fail(c, SPHGPU_ERR_STATE, "force pairs before tree make");
+    const int rc = symmetric_lists(c);
+    if(rc < 0) return rc;
+    return export_lists(c, 1, offsets, ids, cap);
 }
 
 int sphgpu_exhaustive_search(sphgpu_ctx* c, int is_ij, int64_t* offsets, int32_t* ids, int64_t cap)
@@ -772,6 +786,7 @@ int sphgpu_get_counters(sphgpu_ctx* c, sphgpu_counters* o)
     o->walk_split_warps = (int64_t)c->h_status.walk_split_warps;
     o->walk_fallbacks = c->walk_fallbacks;
     o->mlp_guesses = (int64_t)c->h_status.mlp_guesses;
+    o->force_list_builds = c->flist_uses;
     return SPHGPU_OK;
 }
 

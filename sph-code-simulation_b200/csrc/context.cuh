@@ -48,6 +48,13 @@ struct sphgpu_ctx {
     int* d_plist = nullptr;          // symmetric list (FluidForce)
     int* d_pcount = nullptr;
     int64_t pcap = 0;
+    // pair lists built from the gather lists (flist.cu)
+    int* d_tcount = nullptr;         // entries appended to each row from the back
+    int* d_flist_flags = nullptr;    // {incomplete, longest list, over neighborNumber * 1000}
+    double* d_rsearch = nullptr;     // radius of each particle's gather list
+    int flist_n = 0;
+    bool flist_ready = false;        // built for the current tree and h
+    int64_t flist_uses = 0;
 
     // scalars
     double* d_dt = nullptr;          // Simulation::dt
@@ -135,6 +142,12 @@ int gravity(sphgpu_ctx* c, bool direct);
 // Mixed-precision Barnes-Hut walk: FP32 node records of the current tree,
 // then the walk (one launch each).
 int gravity_nodes_mixed(sphgpu_ctx* c);
+// FluidForce's pair lists from the gather lists (flist.cu): save the gather
+// radius before the pre-interaction overwrites h, build after it; the force
+// takes them, or the symmetric tree walk when they are incomplete.
+int save_gather_radius(sphgpu_ctx* c);
+int build_force_lists(sphgpu_ctx* c);
+int symmetric_lists(sphgpu_ctx* c);
 // SRGSPH modules (srgsph.cu), dispatched from the generic ones.
 int sr_pre_interaction(sphgpu_ctx* c);
 int sr_fluid_force(sphgpu_ctx* c);

@@ -1,0 +1,189 @@
+// flist.cu — FluidForce's pair lists built from the gather lists, without a
+// second tree walk.
+//
+// FluidForce sums over the pairs with r < max(h_i, h_j) (src/fluid_force.cpp:
+// 53-60 and the gsph / disph / gdisph forces: the is_ij neighbour search of
+// src/bhtree.cpp:277-316, then the pair test in the force loop).  After the
+// pre-interaction every h is final and, when h_k <= R_k for every particle
+// (R_k the radius of its gather list), those pairs are exactly
+//   own(i)        = { j in gather(i) : r_ij < h_i }
+//   transposed(i) = { j : i in gather(j), r_ij < h_j, not r_ij < h_i }
+// because r < h <= R implies r^2 < R^2 for correctly rounded r = sqrt(r^2),
+// and r_ij = r_ji bit for bit (exact negation, antisymmetric minimum image).
+// Each particle scans its gather list once: own entries go to the front of its
+// row in gather-list order (group ballot compaction), and each pair that only
+// the neighbour's kernel reaches is appended to the neighbour's row from the
+// back (atomic slot).  A finalise pass sorts each row's appended entries by
+// index (a deterministic summation order) and moves them behind the own
+// entries.  If some h_k > R_k, or a row does not fit, the step falls back to
+// the symmetric tree walk, which gives the same pair sets.
+#include <cuda_runtime.h>
+
+#include "context.cuh"
+
+namespace sphgpu {
+
+namespace {
+
+constexpr int LBLK = 256;
+constexpr int LG = 4;  // lanes per particle
+
+__global__ void k_save_radius(const DevState S, int n, double* __restrict__ rs)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < n) rs[i] = S.vel[i].w;
+}
+
+template <int G>
+__global__ void __launch_bounds__(LBLK) k_flist(DevParams P, DevState S, int n, const int* __restrict__ glist,
+                                                const int* __restrict__ gcount, int gcap,
+                                                const double* __restrict__ rs, int* __restrict__ plist,
+                                                int* __restrict__ pcount, int* __restrict__ tcount, int pcap,
+                                                int* __restrict__ flags)
+{
+    constexpr int GPW = 32 / G;
+    const int lane = threadIdx.x & (G - 1);
+    const unsigned gbase = (threadIdx.x & 31) & ~(unsigned)(G - 1);
+    const unsigned gmask = group_mask<G>();
+    const long long warp = ((long long)blockIdx.x * LBLK + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * LBLK) >> 5;
+    for(long long wb = warp * GPW; wb < n; wb += nwarps * GPW) {
+        const int i = (int)(wb + ((threadIdx.x & 31) / G));
+        if(i >= n) continue;  // whole groups drop out together
+        const double4 pi = S.pos[i];
+        const double hi = S.vel[i].w;
+        if(!(hi <= rs[i]) && lane == 0) flags[0] = 1;  // the gather list may miss r < h_i
+        const int cnt = min(gcount[i], gcap);
+        const int* li = glist + (size_t)i * (size_t)gcap;
+        int* row = plist + (size_t)i * (size_t)pcap;
+        int oc = 0;
+        for(int kk = 0; kk < cnt; kk += G) {
+            const int k = kk + lane;
+            bool own = false;
+            int j = 0;
+            if(k < cnt) {
+                j = __ldg(&li[k]);
+                const double4 pj = S.pos[j];
+                const Vec3d d = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
+                const double r = sqrt(abs2x(d));
+                if(r < hi) {
+                    own = true;
+                    if(!(r < __ldg(&S.vel[j].w))) {
+                        // j's own scan does not reach i: append i to j's row
+                        const int t = atomicAdd(&tcount[j], 1);
+                        if(t < pcap) plist[(size_t)j * (size_t)pcap + (pcap - 1 - t)] = i;
+                    }
+                }
+            }
+            const unsigned m = (__ballot_sync(gmask, own) >> gbase) & ((1u << G) - 1u);
+            if(own) {
+                const int pos = oc + __popc(m & ((1u << lane) - 1u));
+                if(pos < pcap) row[pos] = j;
+            }
+            oc += __popc(m);
+        }
+        if(lane == 0) pcount[i] = oc;
+    }
+}
+
+// Appended entries: sorted by index and moved behind the own entries.
+__global__ void k_flist_finalize(int n, int* __restrict__ plist, int* __restrict__ pcount,
+                                 const int* __restrict__ tcount, int pcap, int fatal_limit,
+                                 int* __restrict__ flags)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const int oc = pcount[i], tc = tcount[i];
+    const long long tot = (long long)oc + tc;
+    if(tot > pcap) {
+        flags[0] = 1;
+        return;
+    }
+    if(tot > fatal_limit) flags[2] = 1;
+    int* row = plist + (size_t)i * (size_t)pcap;
+    const int b0 = pcap - tc;
+    for(int a = b0 + 1; a < pcap; ++a) {
+        const int v = row[a];
+        int b = a - 1;
+        while(b >= b0 && row[b] > v) {
+            row[b + 1] = row[b];
+            --b;
+        }
+        row[b + 1] = v;
+    }
+    for(int t = 0; t < tc; ++t) row[oc + t] = row[b0 + t];
+    pcount[i] = (int)tot;
+    atomicMax(&flags[1], (int)tot);
+}
+
+}  // namespace
+
+int build_force_lists(sphgpu_ctx* c)
+{
+    c->flist_ready = false;
+    const int n = c->n;
+    if(n <= 0) return SPHGPU_OK;
+    cudaStream_t st = c->stream;
+    if(c->flist_n < n) return fail(c, SPHGPU_ERR_STATE, "force lists before the gather radius was saved");
+    if(c->pcap < c->gcap) {
+        const int rc = ensure_list_capacity(c, 1, c->gcap);
+        if(rc < 0) return rc;
+    }
+    stage_begin(c, SPHGPU_T_PAIR_WALK);
+    SPHGPU_CUDA(c, cudaMemsetAsync(c->d_tcount, 0, sizeof(int) * (size_t)n, st));
+    SPHGPU_CUDA(c, cudaMemsetAsync(c->d_flist_flags, 0, 3 * sizeof(int), st));
+    const long long gpb = LBLK / LG;
+    const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>((n + gpb - 1) / gpb, 148LL * 8 * 4));
+    k_flist<LG><<<grid, LBLK, 0, st>>>(c->dp, c->s, n, c->d_glist, c->d_gcount, (int)c->gcap, c->d_rsearch,
+                                       c->d_plist, c->d_pcount, c->d_tcount, (int)c->pcap, c->d_flist_flags);
+    k_flist_finalize<<<grid_for(n, 256), 256, 0, st>>>(n, c->d_plist, c->d_pcount, c->d_tcount, (int)c->pcap,
+                                                        c->prm.neighbor_number * 1000, c->d_flist_flags);
+    SPHGPU_LAUNCH_CHECK(c, "force lists");
+    stage_end(c, SPHGPU_T_PAIR_WALK, 2);
+    c->flist_ready = true;
+    return SPHGPU_OK;
+}
+
+int save_gather_radius(sphgpu_ctx* c)
+{
+    if(c->flist_n < c->n) {
+        if(c->d_tcount) cudaFree(c->d_tcount);
+        if(c->d_rsearch) cudaFree(c->d_rsearch);
+        c->d_tcount = nullptr;
+        c->d_rsearch = nullptr;
+        c->flist_n = 0;
+        if(!c->d_flist_flags) SPHGPU_CUDA(c, cudaMalloc(&c->d_flist_flags, 3 * sizeof(int)));
+        SPHGPU_CUDA(c, cudaMalloc(&c->d_tcount, sizeof(int) * (size_t)c->n));
+        SPHGPU_CUDA(c, cudaMalloc(&c->d_rsearch, sizeof(double) * (size_t)c->n));
+        c->flist_n = c->n;
+    }
+    k_save_radius<<<grid_for(c->n, 256), 256, 0, c->stream>>>(c->s, c->n, c->d_rsearch);
+    SPHGPU_LAUNCH_CHECK(c, "gather radius");
+    ++c->launches;  // a copy of n doubles, left out of the stage timers
+    return SPHGPU_OK;
+}
+
+// The pair lists FluidForce sums over: the ones built after the
+// pre-interaction when they are complete (they stay valid until the next tree
+// make), else the symmetric tree walk.
+int symmetric_lists(sphgpu_ctx* c)
+{
+    if(c->flist_ready) {
+        int flags[3] = {0, 0, 0};  // incomplete, longest list, over the limit
+        SPHGPU_CUDA(c, cudaMemcpyAsync(flags, c->d_flist_flags, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+        if(flags[2]) {
+            return fail(c, SPHGPU_ERR_NEIGHBOR_OVERFLOW,
+                        "Neighbor list overflow: more than neighborNumber * 1000 neighbours");
+        }
+        if(!flags[0]) {
+            c->max_pair = flags[1];
+            ++c->flist_uses;
+            return SPHGPU_OK;
+        }
+        c->flist_ready = false;
+    }
+    return pair_walk(c);
+}
+
+}  // namespace sphgpu

@@ -617,7 +617,7 @@ int fluid_force(sphgpu_ctx* c)
     const bool learned = c->prm.riemann_guess == SPHGPU_GUESS_MLP && c->prm.sph_type == SPHGPU_GSPH &&
                          c->prm.riemann_solver == SPHGPU_RIEMANN_ITERATIVE;
     if(learned && !c->have_mlp) return fail(c, SPHGPU_ERR_NO_MLP, "learned Riemann guess requested without MLP weights");
-    const int rc_walk = pair_walk(c);
+    const int rc_walk = symmetric_lists(c);
     if(rc_walk < 0) return rc_walk;
     stage_begin(c, SPHGPU_T_FORCE);
     Harvest hv{c->d_harvest, c->d_harvest_count, c->harvest_cap, c->harvest_mod, 0u};

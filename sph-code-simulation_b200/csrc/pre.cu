@@ -423,6 +423,8 @@ int pre_interaction(sphgpu_ctx* c)
     }
     rc_walk = gather_walk(c, true, c->dp.ratio);
     if(rc_walk < 0) return rc_walk;
+    int rcs = save_gather_radius(c);
+    if(rcs < 0) return rcs;
     stage_begin(c, SPHGPU_T_PRE);
     const double big = DBL_MAX;
     SPHGPU_CUDA(c, cudaMemcpyAsync(c->d_hvs, &big, sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -430,7 +432,9 @@ int pre_interaction(sphgpu_ctx* c)
     else launch_pre<double>(c);
     SPHGPU_LAUNCH_CHECK(c, "PreInteraction");
     stage_end(c, SPHGPU_T_PRE, 1);
-    const int rc = tree_set_kernel(c);
+    int rc = tree_set_kernel(c);
+    if(rc < 0) return rc;
+    rc = build_force_lists(c);
     if(rc < 0) return rc;
     return rc_walk;
 }

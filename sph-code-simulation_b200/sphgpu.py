@@ -134,7 +134,7 @@ class Counters(C.Structure):
     _fields_ = [(n, C.c_int64) for n in (
         "newton_nonconverged", "riemann_solves", "riemann_iterations", "riemann_fallbacks",
         "gather_capacity", "max_gather", "max_pair", "node_count", "retries", "walk_group_warps",
-        "walk_split_warps", "walk_fallbacks", "mlp_guesses")]
+        "walk_split_warps", "walk_fallbacks", "mlp_guesses", "force_list_builds")]
 
 
 _lib = None
@@ -165,6 +165,7 @@ def lib() -> C.CDLL:
         "sphgpu_tree_make": (C.c_int, [vp]),
         "sphgpu_tree_set_kernel": (C.c_int, [vp]),
         "sphgpu_neighbor_search": (C.c_int, [vp, C.c_int, i64p, i32p, i64]),
+        "sphgpu_force_pairs": (C.c_int, [vp, i64p, i32p, i64]),
         "sphgpu_exhaustive_search": (C.c_int, [vp, C.c_int, i64p, i32p, i64]),
         "sphgpu_pre_interaction": (C.c_int, [vp]),
         "sphgpu_fluid_force": (C.c_int, [vp]),
@@ -363,6 +364,16 @@ class Simulation:
         ids = np.zeros(max(int(off[-1]), 1), dtype=np.int32)
         self._check(fn(self._h, int(is_ij), off.ctypes.data_as(i64p), ids.ctypes.data_as(i32p), ids.size),
                     "neighbor_search")
+        return off, ids[: int(off[-1])]
+
+    def force_pairs(self):
+        """The pairs FluidForce sums over now (r < max(h_i, h_j)), CSR in caller order."""
+        off = np.zeros(self.n + 1, dtype=np.int64)
+        i64p, i32p = C.POINTER(C.c_int64), C.POINTER(C.c_int32)
+        self._check(lib().sphgpu_force_pairs(self._h, off.ctypes.data_as(i64p), None, 0), "force_pairs")
+        ids = np.zeros(max(int(off[-1]), 1), dtype=np.int32)
+        self._check(lib().sphgpu_force_pairs(self._h, off.ctypes.data_as(i64p), ids.ctypes.data_as(i32p), ids.size),
+                    "force_pairs")
         return off, ids[: int(off[-1])]
 
     def pre_interaction(self):
