@@ -48,6 +48,31 @@ CASES = {
 }
 
 
+def test_force_lists_when_gather_radius_too_small(gpu):
+    """A density 8x too high makes the gather radius (the guessed h x 1.2) about
+    0.6 of the final h; whichever lists FluidForce then takes, built or walked,
+    hold exactly the pairs r < max(h_i, h_j)."""
+    p = gpu.config_params("evrard_ssph")
+    fields = gpu.sample_evrard(14)
+    with gpu.Simulation(p) as sim:
+        sim.upload(fields)
+        sim.initialize()
+        sim.integrate()
+        st = sim.download()
+        st["dens"] = st["dens"] * 8.0
+        sim.upload(st)
+        sim.set_initial_smoothing(False)
+        sim.tree_make()
+        sim.pre_interaction()
+        off, ids = sim.force_pairs()
+        pos = sim.download(["pos_x", "pos_y", "pos_z", "sml"])
+        woff, wids = sim.neighbor_search(is_ij=True)
+    want = _sets_from_walk(gpu, p, pos, woff, wids)
+    for i in range(len(pos["sml"])):
+        got = ids[off[i]:off[i + 1]]
+        assert len(got) == len(set(got.tolist())) and set(got.tolist()) == want[i], i
+
+
 @pytest.mark.parametrize("case", sorted(CASES))
 def test_force_lists_equal_tree_walk_pairs(gpu, case):
     p, fields = CASES[case](gpu)
