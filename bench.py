@@ -496,7 +496,7 @@ def _cpu_reference(steps: int, warmup: int, workload: str):
     n = len(fields["pos_x"])
     p = wl.params(G, G.FP64)
     p.riemann_guess = G.GUESS_NONE   # the reference has no learned guess
-    sim = cls(p, fields)
+    sim = cls(p, fields, threads=int(os.environ["OMP_NUM_THREADS"])) if kind == "reference" else cls(p, fields)
     sim.initialize()
     for _ in range(warmup):
         sim.integrate()

@@ -101,6 +101,14 @@ typedef struct sphgpu_params {
     /* SRGSPH (SPHParameters::srgsph, include/parameters.hpp:89-96; keys of
      * src/solver.cpp:430-438) */
     int32_t sr_2nd_order;          /* "use2ndOrderSRGSPH" (1)               */
+    int32_t tree_root_origin;      /* non-periodic root cube: 1 = the bounding
+                                      box of the particles and the origin, as
+                                      BHTree::make computes it when OpenMP runs
+                                      more than one thread (its per-thread
+                                      min / max slots other than thread 0's
+                                      start at 0.0: include/openmp.hpp:16-27,
+                                      src/bhtree.cpp:68-91); 0 = the particles'
+                                      own bounding box (one thread).  (1)   */
     double  sr_c_speed;            /* "cSpeed" (1.0)                        */
     double  sr_c_shock;            /* "cShock" (3.0)                        */
     double  sr_c_cd;               /* "cContactDiscontinuity" (1.0)         */

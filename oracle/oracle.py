@@ -93,6 +93,8 @@ def _load(path: str, prefix: str) -> C.CDLL:
         L.oracle_relax_step.argtypes = [vp, dp, dp, dp, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_int, dp]
     else:
         L.ref_create.restype = vp
+        L.ref_set_threads.argtypes = [C.c_int]
+        L.ref_max_threads.restype = C.c_int
         L.ref_create.argtypes = [C.c_void_p, C.c_int64, dpp]
         L.ref_energies.argtypes = [vp, dp, dp, dp]
         L.ref_module_times.argtypes = [vp, dp]
@@ -257,8 +259,15 @@ class Reference(_Base):
 
     prefix = "ref"
 
-    def __init__(self, params, fields: Dict[str, np.ndarray], exhaustive: bool = False):
+    def __init__(self, params, fields: Dict[str, np.ndarray], exhaustive: bool = False, threads: int = 0):
+        """threads: OpenMP team size (0: OMP_NUM_THREADS, else every host
+        core, at least 2).  With one thread BHTree::make's root box is the
+        particles' own bounding box (tree_root_origin = 0); with more it also
+        covers the origin (tree_root_origin = 1)."""
         self.L = _load(REF_EXH_LIB if exhaustive else REF_LIB, "ref")
+        if threads <= 0:
+            threads = int(os.environ.get("OMP_NUM_THREADS", "0") or 0) or max(2, os.cpu_count() or 2)
+        self.L.ref_set_threads(threads)
         self.n = len(fields["pos_x"])
         ptrs, keep = _ptrs(fields, self.n)
         self.h = self.L.ref_create(C.byref(params), self.n, ptrs)

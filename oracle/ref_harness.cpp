@@ -328,6 +328,12 @@ void* ref_create(const sphgpu_params* p, int64_t n, const double* const* fields)
 
 void ref_destroy(void* h) { delete static_cast<RefCtx*>(h); }
 
+// OpenMP team size of the modules.  BHTree::make's bounding box depends on it
+// (more than one thread: the box also covers the origin), and the SRGSPH
+// context sets it to 1 for the whole process.
+void ref_set_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }
+int ref_max_threads(void) { return omp_get_max_threads(); }
+
 const char* ref_last_error(void* h) { return static_cast<RefCtx*>(h)->err.c_str(); }
 
 int ref_get(void* h, double* const* fields)

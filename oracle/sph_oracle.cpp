@@ -234,6 +234,7 @@ struct Node {
 
 struct Tree {
     int max_level = 20, leaf_num = 1;
+    bool root_origin = true;  // non-periodic root box also covers the origin
     std::vector<Node> pool;   // pool[0] is the root
     int used = 0;
     std::vector<int> next;
@@ -346,6 +347,15 @@ struct Tree {
                     const real x = s.f[SPHGPU_F_POS_X + k][i];
                     if(mn[k] > x) mn[k] = x;
                     if(mx[k] < x) mx[k] = x;
+                }
+            }
+            // with more than one OpenMP thread the reference reduces over
+            // per-thread slots that (except thread 0's) start at 0.0
+            // (include/openmp.hpp:16-27, src/bhtree.cpp:68-91)
+            if(root_origin) {
+                for(int k = 0; k < 3; ++k) {
+                    if(mn[k] > 0.0) mn[k] = 0.0;
+                    if(mx[k] < 0.0) mx[k] = 0.0;
                 }
             }
             real l = 0.0;
@@ -1593,6 +1603,7 @@ void* oracle_create(const sphgpu_params* p, int64_t n, const double* const* fiel
         o->per.range[k] = p->range_max[k] - p->range_min[k];
     }
     o->tree.max_level = p->max_tree_level;
+    o->tree.root_origin = p->tree_root_origin != 0;
     o->tree.leaf_num = p->leaf_particle_num;
     o->s.n = (int)n;
     for(int k = 0; k < SPHGPU_NFIELDS; ++k) {

@@ -115,6 +115,7 @@ void set_dev_params(sphgpu_ctx* c)
     d.max_level = p.max_tree_level;
     d.leaf_num = p.leaf_particle_num;
     d.periodic = p.periodic;
+    d.root_origin = p.tree_root_origin;
     for(int k = 0; k < 3; ++k) {
         d.lo[k] = p.range_min[k];
         d.hi[k] = p.range_max[k];
@@ -316,6 +317,7 @@ int check_params(const sphgpu_params* p, std::string& why)
     if(p->neighbor_number <= 0) return why = "neighborNumber must be positive", -1;
     if(p->max_tree_level < 1 || p->max_tree_level > 21) return why = "maxTreeLevel must be in 1..21", -1;
     if(p->leaf_particle_num < 1) return why = "leafParticleNumber must be >= 1", -1;
+    if(p->tree_root_origin != 0 && p->tree_root_origin != 1) return why = "tree_root_origin must be 0 or 1", -1;
     if(p->periodic) {
         for(int k = 0; k < 3; ++k) {
             if(!(p->range_max[k] > p->range_min[k])) return why = "rangeMax must exceed rangeMin", -1;
@@ -363,6 +365,7 @@ void sphgpu_default_params(sphgpu_params* p)
     p->riemann_guess = SPHGPU_GUESS_NONE;
     p->mlp_max_newton = 4;
     p->sr_2nd_order = 1;
+    p->tree_root_origin = 1;
     p->sr_c_speed = 1.0;
     p->sr_c_shock = 3.0;
     p->sr_c_cd = 1.0;

@@ -39,6 +39,7 @@ struct DevParams {
     double alpha_ac;
     int max_level, leaf_num;
     int periodic;
+    int root_origin;  // non-periodic root box also covers the origin
     double lo[3], hi[3], range[3];
     int gravity;
     double G, theta, theta2;

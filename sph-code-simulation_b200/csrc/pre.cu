@@ -178,7 +178,10 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
             }
             if(i != j) {
                 const double vr = dv.x * (vi.x - vj.x) + dv.y * (vi.y - vj.y) + dv.z * (vi.z - vj.z);
-                const double v = ti.w + tj.w - 3.0 * vr * rinv;
+                // coincident particles (r = 0): the reference's vr / r is
+                // 0 / 0, a NaN that never raises v_sig (+-inf if r underflowed)
+                const double v = r > 0.0 ? ti.w + tj.w - 3.0 * vr * rinv
+                                         : (vr < 0.0 ? (double)INFINITY : -(double)INFINITY);
                 if(v > vsig) vsig = v;
             }
             if(need_av || need_grad) {

@@ -100,6 +100,15 @@ __global__ void k_root(const double* __restrict__ part, int nparts, DevParams P,
                 hi[k] = fmax(hi[k], part[b * 6 + 3 + k]);
             }
         }
+        // BHTree::make under more than one OpenMP thread: the min / max
+        // slots of threads other than the first start at 0.0, so the box
+        // reduced from them also covers the origin (src/bhtree.cpp:68-91)
+        if(P.root_origin) {
+            for(int k = 0; k < 3; ++k) {
+                if(lo[k] > 0.0) lo[k] = 0.0;
+                if(hi[k] < 0.0) hi[k] = 0.0;
+            }
+        }
     }
     double c[3], l = 0.0;
     for(int k = 0; k < 3; ++k) {

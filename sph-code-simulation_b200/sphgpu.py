@@ -64,7 +64,7 @@ class Params(C.Structure):
         ("range_min", C.c_double * 3), ("range_max", C.c_double * 3), ("use_gravity", C.c_int32),
         ("gsph_2nd_order", C.c_int32), ("g_constant", C.c_double), ("theta", C.c_double),
         ("riemann_solver", C.c_int32), ("precision", C.c_int32), ("riemann_guess", C.c_int32),
-        ("mlp_max_newton", C.c_int32), ("sr_2nd_order", C.c_int32), ("sr_c_speed", C.c_double),
+        ("mlp_max_newton", C.c_int32), ("sr_2nd_order", C.c_int32), ("tree_root_origin", C.c_int32), ("sr_c_speed", C.c_double),
         ("sr_c_shock", C.c_double), ("sr_c_cd", C.c_double), ("sr_eta", C.c_double), ("sr_c_smooth", C.c_double),
     ]
 

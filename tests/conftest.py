@@ -46,7 +46,10 @@ def golden(name):
 
 def params_from_bytes(G, raw):
     """Parameters stored as raw struct bytes; fields appended to the struct
-    after the fixture was written keep their defaults."""
+    after the fixture was written keep their defaults.  tree_root_origin
+    took over 4 bytes of padding, so fixtures written before it read 0 there
+    (the particles' own root box); their particles span the origin or the box
+    is periodic, where both root boxes are the same."""
     import ctypes
     p = G.default_params()
     b = bytes(raw.tobytes())

@@ -39,6 +39,15 @@ oracle/_ref/libsphref*.so, driven by oracle/ref_harness.cpp):
                      exact SR Riemann solver returns spurious star pressures
                      for nearly equal states, and the primitive recovery then
                      fails), for first / second order and fixed / iterative h.
+  steps_edge_<cfg>.npz
+                     Edge cases, same layout as steps_<cfg> plus the OpenMP
+                     team size the reference ran with: an Evrard sphere moved
+                     off the origin (the non-periodic root box covers the
+                     origin with more than one thread, not with one:
+                     tree_root_origin 1 / 0), three pairs of coincident
+                     particles with different energies (r = 0 pairs), and
+                     1, 2 and 7 particles (smoothing-length Newton without
+                     convergence, a root of one particle).
   lists_<cfg>.npz    Distance-sorted neighbour lists (CSR) from
                      BHTree::neighbor_search and from exhaustive_search
                      (gather and is_ij) at the state after initialize.
@@ -86,6 +95,67 @@ SMALL = {
                                                 range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.1, 0.1)),
                         lambda: G.sample_shock_tube(0.025, ly=0.1)),
 }
+
+
+def _edge_shifted(sph, shift=(1.7, -0.4, 2.3), **kw):
+    fields = G.sample_evrard(8)
+    for k, s in zip(("pos_x", "pos_y", "pos_z"), shift):
+        fields[k] = fields[k] + s
+    return G.config_params(sph, **kw), fields
+
+
+def _edge_coincident():
+    """Three particles moved onto three others; the moved ones get 1.7x the
+    energy, so the coincident pairs differ in pressure and sound speed."""
+    fields = G.sample_evrard(8)
+    rng = np.random.default_rng(7)
+    src = rng.choice(len(fields["pos_x"]), 6, replace=False)
+    for a, b in zip(src[:3], src[3:]):
+        for k in ("pos_x", "pos_y", "pos_z"):
+            fields[k][b] = fields[k][a]
+        fields["ene"][b] = fields["ene"][a] * 1.7
+    return G.config_params("evrard_ssph"), fields
+
+
+def _edge_tiny(n, sph):
+    fields = G.sample_evrard(8)
+    idx = np.random.default_rng(11).choice(len(fields["pos_x"]), n, replace=False)
+    return G.config_params(sph), {k: v[idx].copy() for k, v in fields.items()}
+
+
+# name -> (params and fields, tree_root_origin, reference OpenMP threads)
+EDGE = {
+    "shifted_ssph": (lambda: _edge_shifted("evrard_ssph"), 1, 8),
+    "shifted_ssph_1t": (lambda: _edge_shifted("evrard_ssph"), 0, 1),
+    "shifted_disph": (lambda: _edge_shifted("evrard_disph", neighbor_number=32), 1, 8),
+    "coincident_ssph": (_edge_coincident, 1, 8),
+    "tiny1_ssph": (lambda: _edge_tiny(1, "evrard_ssph"), 1, 8),
+    "tiny2_ssph": (lambda: _edge_tiny(2, "evrard_ssph"), 1, 8),
+    "tiny7_disph": (lambda: _edge_tiny(7, "evrard_disph"), 1, 8),
+}
+
+
+def edge_steps(name, steps=2):
+    mk, origin, threads = EDGE[name]
+    p, fields = mk()
+    p.tree_root_origin = origin
+    ref = O.Reference(p, fields, threads=threads)
+    ref.initialize()
+    states = [ref.download(STATE_FIELDS)]
+    dts = [0.0]
+    for _ in range(steps):
+        ref.integrate()
+        states.append(ref.download(STATE_FIELDS))
+        dts.append(ref.dt)
+    out = {"n": len(fields["pos_x"]), "dt": np.array(dts), "params": np.frombuffer(bytes(p), dtype=np.uint8),
+           "threads": threads}
+    for k in ("pos_x", "pos_y", "pos_z", "vel_x", "vel_y", "vel_z", "mass", "dens", "pres", "ene"):
+        out["ic_" + k] = fields[k]
+    for s, st in enumerate(states):
+        for f, v in st.items():
+            out[f"s{s}_{f}"] = v
+    np.savez_compressed(os.path.join(OUT, f"steps_edge_{name}.npz"), **out)
+    print(f"steps_edge_{name}: n={out['n']} threads={threads} dt={dts}")
 
 
 def evrard_golden():
@@ -316,7 +386,14 @@ def main():
     csv_golden()
     relax_golden()
     sr_golden()
+    for name in EDGE:
+        edge_steps(name)
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["edge"]:
+        O.build(reference=True)
+        for name in EDGE:
+            edge_steps(name)
+    else:
+        main()

@@ -35,11 +35,23 @@ def test_default_params_match_reference_defaults(G):
     assert p.gamma == pytest.approx(5.0 / 3.0, rel=1e-15)
 
 
-def test_params_struct_layout(G):
+def test_params_struct_layout(G, tmp_path):
+    """The ctypes mirror has the C compiler's offsets for every field."""
     import ctypes
-    # offsets of the C struct (natural alignment), checked against ctypes
+    import subprocess
     assert ctypes.sizeof(G.Params) == 240
-    assert G.Params.sr_2nd_order.offset == 192 and G.Params.sr_c_speed.offset == 200
+    assert G.Params.sr_2nd_order.offset == 192 and G.Params.tree_root_origin.offset == 196
+    assert G.Params.sr_c_speed.offset == 200
+    names = [f[0] for f in G.Params._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "sphgpu.h"\nint main(void) {\n'
+                   + "".join(f'    printf("%zu\\n", offsetof(sphgpu_params, {n}));\n' for n in names)
+                   + '    printf("%zu\\n", sizeof(sphgpu_params));\n    return 0;\n}\n')
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert got[:-1] == [getattr(G.Params, n).offset for n in names]
+    assert got[-1] == ctypes.sizeof(G.Params)
 
 
 def test_samples(G):
@@ -70,3 +82,5 @@ def test_bad_params_rejected(G):
         G.Simulation(G.default_params(max_tree_level=30))
     with pytest.raises(G.SPHException, match="kernel"):
         G.Simulation(G.default_params(kernel=7))
+    with pytest.raises(G.SPHException, match="tree_root_origin"):
+        G.Simulation(G.default_params(tree_root_origin=2))

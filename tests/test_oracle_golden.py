@@ -40,6 +40,47 @@ def test_oracle_matches_reference_steps(G, O, name):
             o.integrate()
 
 
+EDGE = ["shifted_ssph", "shifted_ssph_1t", "shifted_disph", "coincident_ssph", "tiny1_ssph", "tiny2_ssph",
+        "tiny7_disph"]
+
+
+@pytest.mark.parametrize("name", EDGE)
+def test_oracle_matches_reference_edge_cases(G, O, name):
+    """Bit-identical states after initialize and two integrate steps on the
+    edge cases: a sphere off the origin with the reference's multi-thread
+    root box (tree_root_origin = 1) and its one-thread box (0), coincident
+    particle pairs, and 1, 2 and 7 particles."""
+    g = golden(f"steps_edge_{name}.npz")
+    p = params_from_bytes(G, g["params"])
+    assert p.tree_root_origin == (0 if int(g["threads"]) == 1 else 1)
+    o = O.Oracle(p, _fields_from_ic(g))
+    o.initialize()
+    for s in range(3):
+        st = o.download()
+        for f in g.files:
+            if f.startswith(f"s{s}_"):
+                np.testing.assert_array_equal(st[f[3:]], g[f], err_msg=f"step {s} field {f[3:]}")
+        if s > 0:
+            assert o.dt == g["dt"][s]
+        if s < 2:
+            o.integrate()
+
+
+def test_root_box_setting_matters_off_origin(G, O):
+    """Off the origin the two root boxes give different trees, and the
+    fixtures of the two reference thread counts differ accordingly."""
+    a, b = golden("steps_edge_shifted_ssph.npz"), golden("steps_edge_shifted_ssph_1t.npz")
+    assert not np.array_equal(a["s0_acc_x"], b["s0_acc_x"])
+    nodes = []
+    for raw in (a["params"], b["params"]):
+        o = O.Oracle(params_from_bytes(G, raw), _fields_from_ic(a))
+        o.tree_make()
+        nodes.append(o.tree_nodes()[1][0])
+    c, e = nodes[0][:3], nodes[0][3]
+    assert np.all(c - 0.5 * e <= 0.0) and np.all(c + 0.5 * e >= 0.0)   # covers the origin
+    assert nodes[1][3] < e
+
+
 def test_oracle_evrard_t0_golden(G, O):
     """Shipped Evrard t=0 snapshot (N=30, Wendland, K=32, leaf=32, TD-AV)."""
     g = golden("evrard_t0.npz")
