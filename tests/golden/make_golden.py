@@ -48,12 +48,22 @@ oracle/_ref/libsphref*.so, driven by oracle/ref_harness.cpp):
                      particles with different energies (r = 0 pairs), and
                      1, 2 and 7 particles (smoothing-length Newton without
                      convergence, a root of one particle).
+  sweep_hashes.json  SHA-256 of the reference's full particle state after
+                     initialize and each of two integrate steps, plus dt, for
+                     56 small configurations: ssph / disph / gsph / gdisph x
+                     cubic / Wendland / Gaussian x leaf 1 / leaf 4 / tree level
+                     cap 3 on an off-origin sphere with gravity, TD-AV and AC;
+                     and a periodic shear layer with particles on the box
+                     faces and one coincident pair, iterative and fixed h,
+                     Balsara off, first-order gsph with the iterative solver.
+                     Inputs are rebuilt from the sweep_* functions below.
   lists_<cfg>.npz    Distance-sorted neighbour lists (CSR) from
                      BHTree::neighbor_search and from exhaustive_search
                      (gather and is_ij) at the state after initialize.
 """
 from __future__ import annotations
 
+import itertools
 import os
 import sys
 
@@ -133,6 +143,75 @@ EDGE = {
     "tiny2_ssph": (lambda: _edge_tiny(2, "evrard_ssph"), 1, 8),
     "tiny7_disph": (lambda: _edge_tiny(7, "evrard_disph"), 1, 8),
 }
+
+
+def sweep_state_hash(st):
+    import hashlib
+    h = hashlib.sha256()
+    for f in STATE_FIELDS:
+        h.update(np.ascontiguousarray(st[f], dtype=np.float64).tobytes())
+    return h.hexdigest()
+
+
+def _sweep_sphere():
+    fields = G.sample_evrard(8)
+    for k, d in zip(("pos_x", "pos_y", "pos_z"), (1.7, -0.4, 2.3)):
+        fields[k] = fields[k] + d
+    return fields
+
+
+def _sweep_layer(iterative):
+    fields = G.sample_shear_layer(0.1, lz=0.125)
+    n = len(fields["pos_x"])
+    idx = np.random.default_rng(3).choice(n, 8, replace=False)
+    fields["pos_x"][idx[:2]] = 0.0                        # on rangeMin
+    fields["pos_y"][idx[2:4]] = 1.0 - 1e-15               # just below rangeMax
+    fields["pos_z"][idx[4:6]] = 0.125 * (1 - 2 ** -52)
+    for k in ("pos_x", "pos_y", "pos_z"):
+        fields[k][idx[6]] = fields[k][idx[7]]             # a coincident pair
+    if not iterative:
+        fields["sml"] = np.full(n, 0.25)
+    return fields
+
+
+def sweep_cases():
+    """name -> (params, fields builder)."""
+    out = {}
+    types = (("ssph", G.SSPH), ("disph", G.DISPH), ("gsph", G.GSPH), ("gdisph", G.GDISPH))
+    for (sph, st), (kern, kn), (leaf, lvl) in itertools.product(
+            types, (("cubic", G.CUBIC_SPLINE), ("wendland", G.WENDLAND), ("gauss", G.GAUSSIAN)),
+            ((1, 20), (4, 20), (1, 3))):
+        p = G.default_params(sph_type=st, kernel=kn, neighbor_number=32, use_gravity=1, g_constant=1.0,
+                             leaf_particle_num=leaf, max_tree_level=lvl, use_time_dependent_av=1, use_ac=1,
+                             riemann_solver=G.RIEMANN_HLL, gamma=5.0 / 3.0)
+        out[f"sphere_{sph}_{kern}_leaf{leaf}_lvl{lvl}"] = (p, _sweep_sphere)
+    variants = (("plain", {}), ("tdav", {"use_balsara_switch": 0, "use_time_dependent_av": 1}),
+                ("first_iter", {"gsph_2nd_order": 0, "riemann_solver": G.RIEMANN_ITERATIVE}))
+    for (sph, st), it, (tag, extra) in itertools.product(types, (1, 0), variants):
+        if tag == "first_iter" and st not in (G.GSPH, G.GDISPH):
+            continue
+        p = G.default_params(sph_type=st, kernel=G.WENDLAND, neighbor_number=32, periodic=1,
+                             range_min=(0.0, 0.0, 0.0), range_max=(1.0, 1.0, 0.125), use_ac=1,
+                             iterative_sml=it, gamma=5.0 / 3.0, **extra)
+        out[f"layer_{sph}_it{it}_{tag}"] = (p, (lambda it=it: _sweep_layer(it)))
+    return out
+
+
+def sweep_golden(steps=2, threads=8):
+    import json
+    rows = []
+    for name, (p, mk) in sweep_cases().items():
+        ref = O.Reference(p, mk(), threads=threads)
+        ref.initialize()
+        hashes, dts = [sweep_state_hash(ref.download(STATE_FIELDS))], [0.0]
+        for _ in range(steps):
+            ref.integrate()
+            hashes.append(sweep_state_hash(ref.download(STATE_FIELDS)))
+            dts.append(ref.dt)
+        rows.append({"name": name, "params": bytes(p).hex(), "threads": threads, "hashes": hashes, "dt": dts})
+    with open(os.path.join(OUT, "sweep_hashes.json"), "w") as f:
+        json.dump(rows, f, indent=1)
+    print(f"sweep_hashes: {len(rows)} configurations")
 
 
 def edge_steps(name, steps=2):
@@ -388,6 +467,7 @@ def main():
     sr_golden()
     for name in EDGE:
         edge_steps(name)
+    sweep_golden()
 
 
 if __name__ == "__main__":
@@ -395,5 +475,6 @@ if __name__ == "__main__":
         O.build(reference=True)
         for name in EDGE:
             edge_steps(name)
+        sweep_golden()
     else:
         main()

@@ -4,10 +4,13 @@ Fixtures in tests/golden/ were produced by the reference's compiled modules
 (tests/golden/make_golden.py); evrard_t0 additionally carries rows of the
 reference's shipped snapshot sample/evrard/results_new/00000.dat.
 """
+import os
+import sys
+
 import numpy as np
 import pytest
 
-from conftest import golden, params_from_bytes
+from conftest import GOLDEN, golden, params_from_bytes
 
 SMALL = ["evrard_ssph", "evrard_ssph_gauss", "evrard_disph", "tube_gsph", "tube_gsph_hll", "shear_disph", "tube_gdisph",
          "tube_gdisph_1st"]
@@ -79,6 +82,36 @@ def test_root_box_setting_matters_off_origin(G, O):
     c, e = nodes[0][:3], nodes[0][3]
     assert np.all(c - 0.5 * e <= 0.0) and np.all(c + 0.5 * e >= 0.0)   # covers the origin
     assert nodes[1][3] < e
+
+
+def _sweep_rows():
+    import json
+    with open(os.path.join(GOLDEN, "sweep_hashes.json")) as f:
+        return json.load(f)
+
+
+SWEEP = _sweep_rows()
+
+
+@pytest.mark.parametrize("row", SWEEP, ids=[r["name"] for r in SWEEP])
+def test_oracle_sweep_matches_reference_hashes(G, O, row):
+    """SHA-256 of the full state after initialize and two steps equals the
+    reference's, over 56 configurations (tests/golden/make_golden.py,
+    sweep_cases): every sph type x kernel x leaf size / tree level cap on an
+    off-origin sphere with gravity, and periodic layers with particles on the
+    box faces and a coincident pair."""
+    sys.path.insert(0, GOLDEN)
+    import make_golden as M
+    p = params_from_bytes(G, np.frombuffer(bytes.fromhex(row["params"]), dtype=np.uint8))
+    _, mk = M.sweep_cases()[row["name"]]
+    o = O.Oracle(p, mk())
+    o.initialize()
+    for s in range(3):
+        assert M.sweep_state_hash(o.download()) == row["hashes"][s], f"step {s}"
+        if s > 0:
+            assert o.dt == row["dt"][s]
+        if s < 2:
+            o.integrate()
 
 
 def test_oracle_evrard_t0_golden(G, O):
