@@ -31,3 +31,28 @@ def test_host_mirror_runs_steps(gpu, tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "neighbours(0)=" in r.stdout
+
+
+def test_reference_side_binding_compiles(tmp_path):
+    """The Module subclasses INTEGRATION.md gives a maintainer compile against
+    the reference's own headers (include/module.hpp, simulation.hpp,
+    parameters.hpp, exception.hpp) and include/sphgpu.h, with the flags the
+    reference's sources build with."""
+    refdir = os.environ.get("REFDIR", "/root/reference")
+    if not os.path.isdir(os.path.join(refdir, "include")):
+        pytest.skip("the reference's headers are not mounted here")
+    lines, inside = [], False
+    for ln in open(os.path.join(ROOT, "INTEGRATION.md")):
+        if ln.startswith("```cpp"):
+            inside = True
+        elif ln.startswith("```"):
+            inside = False
+        elif inside:
+            lines.append(ln)
+    assert lines, "no C++ block in INTEGRATION.md"
+    src = tmp_path / "gpu_modules.cpp"
+    src.write_text("".join(lines))
+    r = subprocess.run(["g++", "-std=c++14", "-fsyntax-only", "-fopenmp", "-DDIM=3", "-include", "string",
+                        "-include", "limits", "-I", os.path.join(refdir, "include"), "-I",
+                        os.path.join(ROOT, "include"), str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
