@@ -115,7 +115,10 @@ def _load(path: str, prefix: str) -> C.CDLL:
             fn.argtypes = [vp, dpp]
         elif name == "neighbor_lists":
             fn.argtypes = [vp, C.c_int, i64p, i32p, C.c_int64]
-        elif name != "destroy":
+        elif name == "destroy":
+            fn.restype = None
+            fn.argtypes = [vp]   # a 64-bit handle: undeclared, ctypes would pass a C int
+        else:
             fn.argtypes = [vp]
     if prefix == "ref":
         L.ref_gravity.argtypes = [vp]

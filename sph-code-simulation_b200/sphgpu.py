@@ -206,6 +206,8 @@ def lib() -> C.CDLL:
         "sphgpu_sample_evrard": (i64, [C.c_int, C.c_double, C.c_double, dpp]),
         "sphgpu_sample_shear_layer": (i64, [C.c_double, C.c_double, C.c_double, dpp]),
         "sphgpu_sample_shock_tube": (i64, [C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, dpp]),
+        "sphgpu_sample_sr_shock_tube": (i64, [C.c_double, C.c_double, C.c_double, C.c_double, dpp]),
+        "sphgpu_timestep_noalloc": (C.c_int, [vp, vp, i64, C.c_double, C.c_double, C.c_double, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

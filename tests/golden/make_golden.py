@@ -49,7 +49,9 @@ oracle/_ref/libsphref*.so, driven by oracle/ref_harness.cpp):
                      1, 2 and 7 particles (smoothing-length Newton without
                      convergence, a root of one particle).
   sweep_hashes.json  SHA-256 of the reference's full particle state after
-                     initialize and each of two integrate steps, plus dt, for
+                     initialize and each of two integrate steps, plus dt and
+                     K, U, W, and of its distance-sorted gather and symmetric
+                     lists after initialize, for
                      56 small configurations: ssph / disph / gsph / gdisph x
                      cubic / Wendland / Gaussian x leaf 1 / leaf 4 / tree level
                      cap 3 on an off-origin sphere with gravity, TD-AV and AC;
@@ -197,6 +199,19 @@ def sweep_cases():
     return out
 
 
+def sweep_lists_hash(sim):
+    """SHA-256 of the distance-sorted gather and symmetric lists (CSR)."""
+    import hashlib
+    out = []
+    for ij in (False, True):
+        off, ids = sim.neighbor_lists(ij)
+        h = hashlib.sha256()
+        h.update(np.ascontiguousarray(off, dtype=np.int64).tobytes())
+        h.update(np.ascontiguousarray(ids, dtype=np.int32).tobytes())
+        out.append(h.hexdigest())
+    return out
+
+
 def sweep_golden(steps=2, threads=8):
     import json
     rows = []
@@ -204,11 +219,15 @@ def sweep_golden(steps=2, threads=8):
         ref = O.Reference(p, mk(), threads=threads)
         ref.initialize()
         hashes, dts = [sweep_state_hash(ref.download(STATE_FIELDS))], [0.0]
+        lists = sweep_lists_hash(ref)
+        energies = [list(ref.energies()[:3])]
         for _ in range(steps):
             ref.integrate()
             hashes.append(sweep_state_hash(ref.download(STATE_FIELDS)))
             dts.append(ref.dt)
-        rows.append({"name": name, "params": bytes(p).hex(), "threads": threads, "hashes": hashes, "dt": dts})
+            energies.append(list(ref.energies()[:3]))
+        rows.append({"name": name, "params": bytes(p).hex(), "threads": threads, "hashes": hashes, "dt": dts,
+                     "lists": lists, "energies": energies})
     with open(os.path.join(OUT, "sweep_hashes.json"), "w") as f:
         json.dump(rows, f, indent=1)
     print(f"sweep_hashes: {len(rows)} configurations")

@@ -84,3 +84,13 @@ def test_bad_params_rejected(G):
         G.Simulation(G.default_params(kernel=7))
     with pytest.raises(G.SPHException, match="tree_root_origin"):
         G.Simulation(G.default_params(tree_root_origin=2))
+
+
+def test_binding_declares_every_entry_point(G):
+    """Every function include/sphgpu.h declares has a ctypes signature in the
+    binding (an undeclared one would pass 64-bit handles as C ints)."""
+    src = open(os.path.join(ROOT, "include", "sphgpu.h")).read()
+    names = set(re.findall(r"\b(sphgpu_\w+)\s*\(", src))
+    L = G.lib()
+    for name in sorted(names):
+        assert getattr(L, name).argtypes is not None, name

@@ -95,19 +95,22 @@ SWEEP = _sweep_rows()
 
 @pytest.mark.parametrize("row", SWEEP, ids=[r["name"] for r in SWEEP])
 def test_oracle_sweep_matches_reference_hashes(G, O, row):
-    """SHA-256 of the full state after initialize and two steps equals the
-    reference's, over 56 configurations (tests/golden/make_golden.py,
-    sweep_cases): every sph type x kernel x leaf size / tree level cap on an
-    off-origin sphere with gravity, and periodic layers with particles on the
-    box faces and a coincident pair."""
+    """SHA-256 of the full state after initialize and two steps, and of the
+    distance-sorted gather and symmetric lists after initialize, equal the
+    reference's; so do dt and K, U, W.  56 configurations
+    (tests/golden/make_golden.py, sweep_cases): every sph type x kernel x leaf
+    size / tree level cap on an off-origin sphere with gravity, and periodic
+    layers with particles on the box faces and a coincident pair."""
     sys.path.insert(0, GOLDEN)
     import make_golden as M
     p = params_from_bytes(G, np.frombuffer(bytes.fromhex(row["params"]), dtype=np.uint8))
     _, mk = M.sweep_cases()[row["name"]]
     o = O.Oracle(p, mk())
     o.initialize()
+    assert M.sweep_lists_hash(o) == row["lists"]
     for s in range(3):
         assert M.sweep_state_hash(o.download()) == row["hashes"][s], f"step {s}"
+        assert list(o.energies()[:3]) == row["energies"][s], f"step {s}"
         if s > 0:
             assert o.dt == row["dt"][s]
         if s < 2:
