@@ -180,6 +180,9 @@ const char* sphgpu_last_error(const sphgpu_ctx* ctx);
 int         sphgpu_device_ok(void);  /* 1 if an sm_100 device is usable */
 
 /* ---------------- state transfer ---------------- */
+/* Largest particle count a context holds: octree nodes (up to 5 n + 2, the
+   reference's pool of BHTree::resize, src/bhtree.cpp:43-51) are int32 indices. */
+#define SPHGPU_MAX_PARTICLES 429496729
 /* fields[k] may be NULL (field zero-filled).  Arrays are length n, in the
    caller's particle order; the caller's index is the particle id.  Device
    buffers are reused when n is unchanged; time, dt and h_per_v_sig persist

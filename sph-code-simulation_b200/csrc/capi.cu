@@ -432,7 +432,8 @@ const char* sphgpu_last_error(const sphgpu_ctx* c) { return c ? c->err.c_str() :
 
 int sphgpu_upload(sphgpu_ctx* c, int64_t n, const double* const* fields)
 {
-    if(!c || n <= 0 || n > (1LL << 30)) return fail(c, SPHGPU_ERR_ARG, "particle count out of range");
+    if(!c || n <= 0 || n > SPHGPU_MAX_PARTICLES)
+        return fail(c, SPHGPU_ERR_ARG, "particle count out of range (1 .. SPHGPU_MAX_PARTICLES)");
     if(!c->stream) return fail(c, SPHGPU_ERR_CUDA, "context has no device");
     if((int)n != c->n || !c->s.pos) {
         int rc = alloc_all(c, (int)n);

@@ -94,3 +94,23 @@ def test_binding_declares_every_entry_point(G):
     L = G.lib()
     for name in sorted(names):
         assert getattr(L, name).argtypes is not None, name
+
+
+def test_particle_count_bounds_checked_first(G):
+    """upload rejects counts its int32 node indices cannot address (5 n + 2
+    nodes) before it touches a device, so this runs with or without one."""
+    import ctypes
+    src = open(os.path.join(ROOT, "include", "sphgpu.h")).read()
+    limit = int(re.search(r"#define SPHGPU_MAX_PARTICLES (\d+)", src).group(1))
+    assert 5 * limit + 2 <= 2 ** 31 - 1 < 5 * (limit + 1) + 2
+    L = G.lib()
+    p = G.default_params()
+    h = ctypes.c_void_p()
+    L.sphgpu_create(ctypes.byref(p), ctypes.byref(h))
+    assert h
+    try:
+        for n in (0, -5, limit + 1):
+            assert L.sphgpu_upload(h, n, None) == -1, n
+            assert b"particle count out of range" in L.sphgpu_last_error(h)
+    finally:
+        L.sphgpu_destroy(h)
