@@ -93,7 +93,8 @@ E2E_IN = ["pos_x", "pos_y", "pos_z", "vel_x", "vel_y", "vel_z", "acc_x", "acc_y"
           "pres", "ene", "dene", "sml", "sound", "balsara", "alpha", "gradh"]
 E2E_OUT = E2E_IN + ["phi", "neighbor"]
 
-# algorithmic bytes per unit (see DESIGN.md "Roofline accounting")
+# algorithmic bytes per unit: each node's link + geo (+ ksize for the symmetric
+# walk) and each particle's position read once, each list entry written once
 NODE_BYTES = 16 + 32          # link (int4) + geo (double4) read per node
 PAIR_WALK_NODE_BYTES = NODE_BYTES + 8
 

@@ -1,7 +1,7 @@
 """CPU FP64 oracle of the learned Riemann guess (TEST INFRASTRUCTURE ONLY).
 
 The network has no counterpart in the reference; this file is the CPU
-judge of the project's tensor-core kernels: features, forward pass, loss and
+checker of the project's tensor-core kernels: features, forward pass, loss and
 the full backward pass in float64 numpy.  With bf16=True it rounds weights,
 inputs, hidden activations and back-propagated pre-activation gradients to
 bfloat16 at the points where the GPU kernels do, so the remaining difference

@@ -34,8 +34,9 @@ def test_host_mirror_runs_steps(gpu, tmp_path):
 
 
 def test_reference_side_binding_compiles(tmp_path):
-    """The Module subclasses INTEGRATION.md gives a maintainer compile against
-    the reference's own headers (include/module.hpp, simulation.hpp,
+    """The Module subclasses of the integration guide (its C++ block, what a
+    maintainer adds beside src/solver.cpp) compile against the reference's
+    own headers (include/module.hpp, simulation.hpp,
     parameters.hpp, exception.hpp) and include/sphgpu.h, with the flags the
     reference's sources build with."""
     refdir = os.environ.get("REFDIR", "/root/reference")
@@ -49,7 +50,7 @@ def test_reference_side_binding_compiles(tmp_path):
             inside = False
         elif inside:
             lines.append(ln)
-    assert lines, "no C++ block in INTEGRATION.md"
+    assert lines, "no C++ block in the integration guide"
     src = tmp_path / "gpu_modules.cpp"
     src.write_text("".join(lines))
     r = subprocess.run(["g++", "-std=c++14", "-fsyntax-only", "-fopenmp", "-DDIM=3", "-include", "string",
