@@ -17,6 +17,11 @@ oracle/_ref/libsphref*.so, driven by oracle/ref_harness.cpp):
                      printed 6 digits, then stores every 16th particle's printed
                      row, the recomputed full-precision values for the same
                      particles, and W0.
+  evrard_energy.json The rows of the reference's shipped
+                     sample/evrard/results_new/energy.dat (time, kinetic,
+                     thermal, potential, total; same configuration as
+                     evrard_t0).  An older build of the reference wrote them,
+                     so later rows bound a run (~1e-2), they do not pin it.
   steps_<cfg>.npz    Small instances of the benchmark workloads (and of the
                      gdisph shock tube, first and second order, and of the
                      ssph Evrard sphere with the Gaussian kernel): the
@@ -107,6 +112,15 @@ SMALL = {
                                                 range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.1, 0.1)),
                         lambda: G.sample_shock_tube(0.025, ly=0.1)),
 }
+
+
+def evrard_energy_golden():
+    import json
+    rows = np.loadtxt(os.path.join(REFDIR, "sample/evrard/results_new/energy.dat"), comments="#")
+    with open(os.path.join(OUT, "evrard_energy.json"), "w") as f:
+        json.dump({"columns": ["time", "kinetic", "thermal", "potential", "total"],
+                   "rows": [[float(x) for x in r] for r in rows]}, f, indent=1)
+    print(f"evrard_energy: {len(rows)} rows")
 
 
 def _edge_shifted(sph, shift=(1.7, -0.4, 2.3), **kw):
@@ -477,6 +491,7 @@ def main():
     if not O.have_reference():
         raise SystemExit("reference libraries not built; is REFDIR mounted?")
     evrard_golden()
+    evrard_energy_golden()
     for name in SMALL:
         small_steps(name)
     for name in ("evrard_ssph", "tube_gsph", "shear_disph"):

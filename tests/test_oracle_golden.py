@@ -137,6 +137,29 @@ def test_oracle_evrard_t0_golden(G, O):
     assert abs(w - float(g["w0_printed"])) < 1e-6
 
 
+def test_oracle_evrard_energy_to_t1_within_shipped_bounds(G, O):
+    """The shipped Evrard run (sample/evrard/results_new/energy.dat, same
+    configuration as the t = 0 snapshot) integrated to t = 1 (~400 steps).
+    An older build of the reference wrote that file, so the check is a bound,
+    not parity: K, U, W within 1e-2 and the total within 1e-3 of its t = 1.00048
+    row (measured: 4.6e-3, 2.1e-3, 6.3e-4 and 6.1e-5)."""
+    import json
+    with open(os.path.join(GOLDEN, "evrard_energy.json")) as f:
+        t_ref, k_ref, u_ref, w_ref, e_ref = json.load(f)["rows"][1]
+    p = G.default_params(sph_type=G.SSPH, kernel=G.WENDLAND, neighbor_number=32, leaf_particle_num=32,
+                         use_balsara_switch=1, use_time_dependent_av=1, av_alpha=1.0, use_gravity=1,
+                         g_constant=1.0, gamma=1.66666666666666666667, cfl_sound=0.2, cfl_force=0.1)
+    o = O.Oracle(p, G.sample_evrard(30))
+    o.initialize()
+    while o.time < 1.0:
+        o.integrate()
+    assert abs(o.time - t_ref) < 5e-3
+    k, u, w, _ = o.energies()
+    for got, ref in ((k, k_ref), (u, u_ref), (w, w_ref)):
+        assert abs(got - ref) <= 1e-2 * abs(ref), (got, ref)
+    assert abs(k + u + w - e_ref) <= 1e-3 * abs(e_ref)
+
+
 @pytest.mark.parametrize("name", ["evrard_ssph", "tube_gsph", "shear_disph"])
 def test_oracle_neighbor_lists(G, O, name):
     """Distance-sorted lists equal the reference's tree and exhaustive lists."""
