@@ -158,6 +158,16 @@ typedef struct sphgpu_counters {
     int64_t mlp_guesses;           /* pairs whose start came from the network */
     int64_t force_list_builds;     /* FluidForce calls that took the pair lists
                                       built from the gather lists (no walk) */
+    /* work done since the last reset, the units of the FLOP roofline */
+    int64_t pre_candidates;        /* gather-list entries tested, summed over
+                                      the Newton sweeps and the final pass  */
+    int64_t pre_newton_pairs;      /* pairs inside h in the Newton sweeps    */
+    int64_t pre_pairs;             /* pairs inside h in the final pass       */
+    int64_t force_candidates;      /* pair-list entries tested by FluidForce */
+    int64_t force_pairs;           /* pairs inside max(h_i, h_j)             */
+    int64_t gravity_nodes;         /* tree nodes met (opening tests)         */
+    int64_t gravity_monopoles;     /* nodes taken as monopoles               */
+    int64_t gravity_leaf_pairs;    /* softened particle pairs                */
 } sphgpu_counters;
 
 /* Stage timers (ms, summed since the last reset; CUDA events on the
@@ -328,7 +338,18 @@ int sphgpu_reset_counters(sphgpu_ctx* ctx);
 int sphgpu_enable_timing(sphgpu_ctx* ctx, int on);
 int sphgpu_get_stage_times(sphgpu_ctx* ctx, double* ms /* [SPHGPU_NSTAGES] */,
                            int64_t* launches /* [SPHGPU_NSTAGES] or NULL */);
+/* Wait for the context's stream.  Also reports (SPHGPU_ERR_STATE) a bound
+   hit since the last wait by a device pass that runs without a host wait of
+   its own: the bottom-up mass and kernel_size passes and the gravity walks,
+   which bound their loops by the tree depth and node count instead of
+   looping on a corrupt tree.  sphgpu_integrate, sphgpu_initialize and the
+   next tree_make / neighbour walk report it the same way. */
 int sphgpu_synchronize(sphgpu_ctx* ctx);
+/* Test hook: set PASS_GUARD bits (1 mass, 2 set_kernel, 4 gravity, 8 mixed
+   gravity) on the device as those passes do when they hit their bound, so a
+   test can check that the next synchronising call reports it without
+   corrupting a tree.  No counterpart in the reference. */
+int sphgpu_test_flag_pass_guard(sphgpu_ctx* ctx, int bits);
 /* CUDA-event timer on the context stream: elapsed device time between the
    two calls (the stop call waits for the stream). */
 int sphgpu_timer_start(sphgpu_ctx* ctx);
@@ -349,7 +370,9 @@ int64_t sphgpu_launch_count(const sphgpu_ctx* ctx);
    SPHGPU_NOALLOC_MAX_PARTICLES is rejected with SPHGPU_ERR_ARG.  The first
    call on a device looks up the array's device address (make it before any
    stream capture).  All calls share the array: calls that overlap on the GPU
-   race. */
+   race.  The looked-up address is cached per device for the life of the
+   process: do not call this entry point again after cudaDeviceReset on that
+   device (the cached address would then be stale). */
 #define SPHGPU_NOALLOC_TILE 1024
 #define SPHGPU_NOALLOC_MAX_BLOCKS 4096
 #define SPHGPU_NOALLOC_MAX_PARTICLES (SPHGPU_NOALLOC_TILE * SPHGPU_NOALLOC_MAX_BLOCKS)

@@ -28,6 +28,29 @@ int cuda_fail(sphgpu_ctx* c, cudaError_t e, const char* where)
     return fail(c, SPHGPU_ERR_CUDA, m);
 }
 
+int check_pass_guard(sphgpu_ctx* c)
+{
+    const int bits = c->h_status.pass_guard;
+    if(!bits) return SPHGPU_OK;
+    c->h_status.pass_guard = 0;
+    SPHGPU_CUDA(c, cudaMemsetAsync(&c->d_status->pass_guard, 0, sizeof(int), c->stream));
+    std::string m = "a bounded device pass hit its limit (corrupt tree):";
+    if(bits & PASS_GUARD_MASS) m += " mass / centre of mass";
+    if(bits & PASS_GUARD_KSIZE) m += " set_kernel";
+    if(bits & PASS_GUARD_GRAVITY) m += " gravity walk";
+    if(bits & PASS_GUARD_GRAVITY32) m += " mixed gravity walk";
+    return fail(c, SPHGPU_ERR_STATE, m);
+}
+
+int sync_and_check(sphgpu_ctx* c)
+{
+    if(c->d_status)
+        SPHGPU_CUDA(c, cudaMemcpyAsync(&c->h_status.pass_guard, &c->d_status->pass_guard, sizeof(int),
+                                       cudaMemcpyDeviceToHost, c->stream));
+    SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    return c->d_status ? check_pass_guard(c) : SPHGPU_OK;
+}
+
 static cudaEvent_t take_event(sphgpu_ctx* c)
 {
     if(c->ev_pool.empty()) {
@@ -141,6 +164,9 @@ void free_all(sphgpu_ctx* c)
     if(c->d_plist) cudaFree(c->d_plist);
     c->d_glist = c->d_plist = nullptr;
     c->gcap = c->pcap = 0;
+    if(c->d_stage) cudaFree(c->d_stage);
+    c->d_stage = nullptr;
+    c->stage_cap = 0;
 }
 
 template <typename T>
@@ -251,37 +277,109 @@ FieldRef field_ref(const DevState& s, int f)
     }
 }
 
-__device__ __forceinline__ double& comp_of(double4& v, int c)
-{
-    return c == 0 ? v.x : (c == 1 ? v.y : (c == 2 ? v.z : v.w));
-}
+// Device sources of one upload / destinations of one download: a staging slot
+// per field, or null (upload: the field is set to 0; download: not read).
+struct FieldSlots {
+    double* p[SPHGPU_NFIELDS];
+};
 
-__global__ void k_put(double4* __restrict__ arr, int comp, const double* __restrict__ src, int n)
+// Upload: every record of particle i (caller order = octree order until the
+// next tree_make) written whole from the staged fields, in one pass.
+__global__ void k_put_all(DevState S, FieldSlots F, int n)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if(i < n) comp_of(arr[i], comp) = src ? src[i] : 0.0;
-}
-
-__global__ void k_put_nbr(int* __restrict__ nbr, const double* __restrict__ src, int n)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if(i < n) nbr[i] = src ? (int)src[i] : 0;
-}
-
-__global__ void k_get(const double4* __restrict__ arr, int comp, const int* __restrict__ id, double* __restrict__ dst,
-                      int n)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if(i < n) {
-        double4 v = arr[i];
-        dst[id[i]] = comp_of(v, comp);
+    if(i >= n) return;
+    auto g = [&](int f) { return F.p[f] ? F.p[f][i] : 0.0; };
+    S.pos[i] = make_double4(g(SPHGPU_F_POS_X), g(SPHGPU_F_POS_Y), g(SPHGPU_F_POS_Z), g(SPHGPU_F_MASS));
+    S.vel[i] = make_double4(g(SPHGPU_F_VEL_X), g(SPHGPU_F_VEL_Y), g(SPHGPU_F_VEL_Z), g(SPHGPU_F_SML));
+    S.acc[i] = make_double4(g(SPHGPU_F_ACC_X), g(SPHGPU_F_ACC_Y), g(SPHGPU_F_ACC_Z), g(SPHGPU_F_DENE));
+    S.velp[i] = make_double4(g(SPHGPU_F_VELP_X), g(SPHGPU_F_VELP_Y), g(SPHGPU_F_VELP_Z), g(SPHGPU_F_ENE_P));
+    S.thermo[i] = make_double4(g(SPHGPU_F_DENS), g(SPHGPU_F_PRES), g(SPHGPU_F_ENE), g(SPHGPU_F_SOUND));
+    S.visc[i] = make_double4(g(SPHGPU_F_ALPHA), g(SPHGPU_F_BALSARA), g(SPHGPU_F_GRADH), g(SPHGPU_F_PHI));
+    S.nbr[i] = (int)g(SPHGPU_F_NEIGHBOR);
+    S.id[i] = i;
+    const size_t m = (size_t)n;
+    for(int q = 0; q < 4; ++q) {
+        const int f = SPHGPU_F_GRAD_D_X + 4 * q;
+        S.grad[q * m + i] = make_double4(g(f), g(f + 1), g(f + 2), q < 3 ? g(f + 3) : 0.0);
+    }
+    if(S.sr) {
+        for(int q = 0; q < 3; ++q) {
+            const int f = SPHGPU_F_SR_S_X + 4 * q;
+            S.sr[q * m + i] = make_double4(g(f), g(f + 1), g(f + 2), g(f + 3));
+        }
     }
 }
 
-__global__ void k_get_nbr(const int* __restrict__ nbr, const int* __restrict__ id, double* __restrict__ dst, int n)
+// Download: each requested field of particle i into its slot at the caller's
+// index id[i], in one pass.
+__global__ void k_get_all(DevState S, FieldSlots F, int n)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if(i < n) dst[id[i]] = (double)nbr[i];
+    if(i >= n) return;
+    const int dst = S.id[i];
+    auto put4 = [&](int f0, double4 v) {
+        if(F.p[f0]) F.p[f0][dst] = v.x;
+        if(F.p[f0 + 1]) F.p[f0 + 1][dst] = v.y;
+        if(F.p[f0 + 2]) F.p[f0 + 2][dst] = v.z;
+    };
+    auto put1 = [&](int f, double v) {
+        if(F.p[f]) F.p[f][dst] = v;
+    };
+    const double4 pos = S.pos[i], vel = S.vel[i], acc = S.acc[i], velp = S.velp[i], th = S.thermo[i],
+                  vs = S.visc[i];
+    put4(SPHGPU_F_POS_X, pos);
+    put1(SPHGPU_F_MASS, pos.w);
+    put4(SPHGPU_F_VEL_X, vel);
+    put1(SPHGPU_F_SML, vel.w);
+    put4(SPHGPU_F_ACC_X, acc);
+    put1(SPHGPU_F_DENE, acc.w);
+    put4(SPHGPU_F_VELP_X, velp);
+    put1(SPHGPU_F_ENE_P, velp.w);
+    put1(SPHGPU_F_DENS, th.x);
+    put1(SPHGPU_F_PRES, th.y);
+    put1(SPHGPU_F_ENE, th.z);
+    put1(SPHGPU_F_SOUND, th.w);
+    put1(SPHGPU_F_ALPHA, vs.x);
+    put1(SPHGPU_F_BALSARA, vs.y);
+    put1(SPHGPU_F_GRADH, vs.z);
+    put1(SPHGPU_F_PHI, vs.w);
+    put1(SPHGPU_F_NEIGHBOR, (double)S.nbr[i]);
+    const size_t m = (size_t)n;
+    for(int q = 0; q < 4; ++q) {
+        const int f = SPHGPU_F_GRAD_D_X + 4 * q;
+        const double4 v = S.grad[q * m + i];
+        put1(f, v.x);
+        put1(f + 1, v.y);
+        put1(f + 2, v.z);
+        if(q < 3) put1(f + 3, v.w);
+    }
+    if(S.sr) {
+        for(int q = 0; q < 3; ++q) {
+            const int f = SPHGPU_F_SR_S_X + 4 * q;
+            const double4 v = S.sr[q * m + i];
+            put1(f, v.x);
+            put1(f + 1, v.y);
+            put1(f + 2, v.z);
+            put1(f + 3, v.w);
+        }
+    }
+}
+
+// Staging for `slots` fields of n doubles, grown on demand and kept.
+int ensure_stage(sphgpu_ctx* c, int slots)
+{
+    const int64_t want = (int64_t)slots * c->n;
+    if(want <= c->stage_cap && c->d_stage) return SPHGPU_OK;
+    if(c->d_stage) {
+        SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+        SPHGPU_CUDA(c, cudaFree(c->d_stage));
+        c->d_stage = nullptr;
+        c->stage_cap = 0;
+    }
+    SPHGPU_CUDA(c, cudaMalloc(&c->d_stage, sizeof(double) * (size_t)std::max<int64_t>(want, 1)));
+    c->stage_cap = want;
+    return SPHGPU_OK;
 }
 
 // Solver::initialize (src/solver.cpp:941-953)
@@ -439,18 +537,24 @@ int sphgpu_upload(sphgpu_ctx* c, int64_t n, const double* const* fields)
         int rc = alloc_all(c, (int)n);
         if(rc) return rc;
     }
-    double* stage = nullptr;
-    SPHGPU_CUDA(c, cudaMallocAsync(&stage, sizeof(double) * (size_t)n, c->stream));
-    const unsigned g = grid_for(n, 256);
+    // every given field to its own staging slot (back-to-back copies on the
+    // stream: DMA at the link rate from pinned buffers), then one pass that
+    // writes every particle record whole
+    // (srgsph fields are kept only by srgsph contexts)
+    auto wanted = [&](int f) { return fields && fields[f] && (f < SPHGPU_F_SR_S_X || c->s.sr); };
+    int slots = 0;
+    for(int f = 0; f < SPHGPU_NFIELDS; ++f) slots += wanted(f) ? 1 : 0;
+    int rc = ensure_stage(c, slots);
+    if(rc) return rc;
+    FieldSlots F{};
+    int k = 0;
     for(int f = 0; f < SPHGPU_NFIELDS; ++f) {
-        const double* src = fields ? fields[f] : nullptr;
-        if(src) SPHGPU_CUDA(c, cudaMemcpyAsync(stage, src, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
-        const FieldRef r = field_ref(c->s, f);
-        if(r.comp == 4) k_put_nbr<<<g, 256, 0, c->stream>>>(c->s.nbr, src ? stage : nullptr, (int)n);
-        else if(r.arr) k_put<<<g, 256, 0, c->stream>>>(r.arr, r.comp, src ? stage : nullptr, (int)n);
+        if(!wanted(f)) continue;
+        F.p[f] = c->d_stage + (size_t)k++ * (size_t)n;
+        SPHGPU_CUDA(c, cudaMemcpyAsync(F.p[f], fields[f], sizeof(double) * (size_t)n, cudaMemcpyHostToDevice,
+                                       c->stream));
     }
-    k_iota<<<g, 256, 0, c->stream>>>(c->s.id, (int)n);
-    SPHGPU_CUDA(c, cudaFreeAsync(stage, c->stream));
+    k_put_all<<<grid_for(n, 256), 256, 0, c->stream>>>(c->s, F, (int)n);
     SPHGPU_LAUNCH_CHECK(c, "upload");
     SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
     c->have_tree = false;
@@ -465,22 +569,32 @@ int sphgpu_download(sphgpu_ctx* c, double* const* fields)
     if(!c || !fields) return SPHGPU_ERR_ARG;
     if(c->n <= 0) return fail(c, SPHGPU_ERR_STATE, "no particles uploaded");
     const int n = c->n;
-    double* stage = nullptr;
-    SPHGPU_CUDA(c, cudaMallocAsync(&stage, sizeof(double) * (size_t)n, c->stream));
-    const unsigned g = grid_for(n, 256);
+    int slots = 0;
     for(int f = 0; f < SPHGPU_NFIELDS; ++f) {
         if(!fields[f]) continue;
-        const FieldRef r = field_ref(c->s, f);
-        if(r.comp != 4 && !r.arr) {  // srgsph fields of another SPH type: zeros
+        if(f >= SPHGPU_F_SR_S_X && !c->s.sr) {  // srgsph fields of another SPH type: zeros
             std::fill(fields[f], fields[f] + n, 0.0);
             continue;
         }
-        if(r.comp == 4) k_get_nbr<<<g, 256, 0, c->stream>>>(c->s.nbr, c->s.id, stage, n);
-        else k_get<<<g, 256, 0, c->stream>>>(r.arr, r.comp, c->s.id, stage, n);
-        SPHGPU_CUDA(c, cudaMemcpyAsync(fields[f], stage, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+        ++slots;
     }
-    SPHGPU_CUDA(c, cudaFreeAsync(stage, c->stream));
+    int rc = ensure_stage(c, slots);
+    if(rc) return rc;
+    FieldSlots F{};
+    int k = 0;
+    for(int f = 0; f < SPHGPU_NFIELDS; ++f) {
+        if(!fields[f] || (f >= SPHGPU_F_SR_S_X && !c->s.sr)) continue;
+        F.p[f] = c->d_stage + (size_t)k++ * (size_t)n;
+    }
+    // one pass fills every requested slot in caller order, then the slots go
+    // back to back over the link; one wait at the end
+    k_get_all<<<grid_for(n, 256), 256, 0, c->stream>>>(c->s, F, n);
     SPHGPU_LAUNCH_CHECK(c, "download");
+    for(int f = 0; f < SPHGPU_NFIELDS; ++f) {
+        if(!F.p[f]) continue;
+        SPHGPU_CUDA(c, cudaMemcpyAsync(fields[f], F.p[f], sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost,
+                                       c->stream));
+    }
     SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
     return SPHGPU_OK;
 }
@@ -625,8 +739,7 @@ int sphgpu_initialize(sphgpu_ctx* c)
     if(rc < 0) return rc;
     rc = gravity(c, false);
     if(rc < 0) return rc;
-    SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
-    return SPHGPU_OK;
+    return sync_and_check(c);
 }
 
 int sphgpu_integrate(sphgpu_ctx* c)
@@ -642,8 +755,9 @@ int sphgpu_integrate(sphgpu_ctx* c)
     if((rc = fluid_force(c)) < 0) return rc;
     if((rc = gravity(c, false)) < 0) return rc;
     if((rc = correct(c)) < 0) return rc;
-    SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+    rc = sync_and_check(c);
     stage_flush(c);
+    if(rc < 0) return rc;
     c->time += dt_h;
     return SPHGPU_OK;
 }
@@ -791,6 +905,14 @@ int sphgpu_get_counters(sphgpu_ctx* c, sphgpu_counters* o)
     o->walk_fallbacks = c->walk_fallbacks;
     o->mlp_guesses = (int64_t)c->h_status.mlp_guesses;
     o->force_list_builds = c->flist_uses;
+    o->pre_candidates = (int64_t)c->h_status.pre_cand;
+    o->pre_newton_pairs = (int64_t)c->h_status.pre_newton_pairs;
+    o->pre_pairs = (int64_t)c->h_status.pre_pairs;
+    o->force_candidates = (int64_t)c->h_status.force_cand;
+    o->force_pairs = (int64_t)c->h_status.force_pairs;
+    o->gravity_nodes = (int64_t)c->h_status.grav_nodes;
+    o->gravity_monopoles = (int64_t)c->h_status.grav_mono;
+    o->gravity_leaf_pairs = (int64_t)c->h_status.grav_leaf_pairs;
     return SPHGPU_OK;
 }
 
@@ -855,6 +977,13 @@ int64_t sphgpu_launch_count(const sphgpu_ctx* c) { return c ? c->launches : 0; }
 int sphgpu_synchronize(sphgpu_ctx* c)
 {
     if(!c || !c->stream) return SPHGPU_ERR_ARG;
+    return sync_and_check(c);
+}
+
+int sphgpu_test_flag_pass_guard(sphgpu_ctx* c, int bits)
+{
+    if(!c || !c->d_status || bits <= 0 || bits > 15) return SPHGPU_ERR_ARG;
+    SPHGPU_CUDA(c, cudaMemcpyAsync(&c->d_status->pass_guard, &bits, sizeof(int), cudaMemcpyHostToDevice, c->stream));
     SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
     return SPHGPU_OK;
 }

@@ -85,8 +85,9 @@ struct DevStatus {
     int fatal;             // a list exceeded neighbor_number * 1000
     int max_count;         // largest list seen
     int node_pool;         // node pool exhausted
-    int guard;             // a bounded device loop hit its limit (corrupt tree)
+    int guard;             // a neighbour walk hit its node-count bound (corrupt tree)
     int nonfinite;         // a particle position is NaN or infinite
+    int pass_guard;        // PASS_GUARD_* bits: a bottom-up pass or gravity walk hit its bound
     unsigned long long newton_nonconv;
     unsigned long long riemann_solves;
     unsigned long long riemann_iters;
@@ -95,7 +96,43 @@ struct DevStatus {
     unsigned long long walk_split_warps;   // warps walked as several sub-groups
     unsigned long long mlp_guesses;        // pairs sent to the learned guess
     int sr_recovery;                       // srgsph: a Lorentz-factor solve did not converge
+    // work counters (units of the FLOP roofline; reset with the others)
+    unsigned long long pre_cand;           // gather-list candidates tested (every sweep + fused pass)
+    unsigned long long pre_newton_pairs;   // pairs inside h in the Newton sweeps
+    unsigned long long pre_pairs;          // pairs inside h in the fused pass
+    unsigned long long force_cand;         // pair-list entries tested by FluidForce
+    unsigned long long force_pairs;        // pairs inside max(h_i, h_j)
+    unsigned long long grav_nodes;         // nodes met by the gravity walk (opening tests)
+    unsigned long long grav_mono;          // nodes accepted as monopoles
+    unsigned long long grav_leaf_pairs;    // softened particle pairs in opened leaves
 };
+
+// Sum a per-lane work counter over the block and add it to a device total
+// (one atomic per block).  Every thread of the block must call it.
+__device__ __forceinline__ void block_count(unsigned long long* total, unsigned v)
+{
+    __shared__ unsigned long long s_cnt[32];
+    unsigned long long x = v;
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    const int w = threadIdx.x >> 5;
+    __syncthreads();
+    if((threadIdx.x & 31) == 0) s_cnt[w] = x;
+    __syncthreads();
+    if(threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for(int k = 0; k < (int)((blockDim.x + 31) >> 5); ++k) t += s_cnt[k];
+        if(t) atomicAdd(total, t);
+    }
+}
+
+// Bits of DevStatus::pass_guard.  The passes that set them run without a
+// host wait after them; the host reports the bit at its next wait on the
+// stream (check_pass_guard in capi.cu).
+constexpr int PASS_GUARD_MASS = 1;       // bottom-up mass / centre of mass
+constexpr int PASS_GUARD_KSIZE = 2;      // bottom-up kernel_size (set_kernel)
+constexpr int PASS_GUARD_GRAVITY = 4;    // Barnes-Hut walk (FP64)
+constexpr int PASS_GUARD_GRAVITY32 = 8;  // Barnes-Hut walk (mixed form)
 
 // Read-only 32-byte load through the non-coherent path (two 16-byte halves).
 __device__ __forceinline__ double4 ldg4(const double4* p)

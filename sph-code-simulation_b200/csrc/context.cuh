@@ -56,6 +56,11 @@ struct sphgpu_ctx {
     bool flist_ready = false;        // built for the current tree and h
     int64_t flist_uses = 0;
 
+    // host transfer staging (upload / download): one slot of n doubles per
+    // field moved, kept across calls
+    double* d_stage = nullptr;
+    int64_t stage_cap = 0;           // doubles d_stage holds
+
     // scalars
     double* d_dt = nullptr;          // Simulation::dt
     double* d_hvs = nullptr;         // Simulation::h_per_v_sig
@@ -124,6 +129,40 @@ int cuda_fail(sphgpu_ctx* c, cudaError_t e, const char* where);
         if(e_ != cudaSuccess) return cuda_fail((c), e_, (where)); \
     } while(0)
 
+// Device temporaries of one call, released on every return path (error
+// returns included): stream-ordered with cudaFreeAsync when taken with
+// cudaMallocAsync on the stream, else with cudaFree.
+class DevTemps {
+public:
+    explicit DevTemps(cudaStream_t s) : s_(s) {}
+    ~DevTemps()
+    {
+        for(const Item& a : items_) {
+            if(a.async) cudaFreeAsync(a.p, s_);
+            else cudaFree(a.p);
+        }
+    }
+    DevTemps(const DevTemps&) = delete;
+    DevTemps& operator=(const DevTemps&) = delete;
+    template <typename T>
+    cudaError_t get(T** p, size_t bytes, bool async = true)
+    {
+        void* q = nullptr;
+        const cudaError_t e = async ? cudaMallocAsync(&q, bytes, s_) : cudaMalloc(&q, bytes);
+        if(e == cudaSuccess) items_.push_back({q, async});
+        *p = static_cast<T*>(q);
+        return e;
+    }
+
+private:
+    struct Item {
+        void* p;
+        bool async;
+    };
+    cudaStream_t s_;
+    std::vector<Item> items_;
+};
+
 // stage timers
 void stage_begin(sphgpu_ctx* c, int stage);
 void stage_end(sphgpu_ctx* c, int stage, int launches);
@@ -159,7 +198,14 @@ int timestep(sphgpu_ctx* c);
 int predict(sphgpu_ctx* c);
 int correct(sphgpu_ctx* c);
 int energies(sphgpu_ctx* c, double* out5 /* K, U, W, px.. */);
-int read_status(sphgpu_ctx* c);
+// Report a bound hit by a pass that ran without a host wait after it (mass,
+// set_kernel, gravity): call after a wait that copied DevStatus::pass_guard
+// into h_status.  Clears the word on the device and returns SPHGPU_ERR_STATE
+// when a bit is set, SPHGPU_OK otherwise.
+int check_pass_guard(sphgpu_ctx* c);
+// Copy DevStatus::pass_guard to the host, wait on the stream, then
+// check_pass_guard.
+int sync_and_check(sphgpu_ctx* c);
 int ensure_list_capacity(sphgpu_ctx* c, int which, int64_t cap);
 
 }  // namespace sphgpu

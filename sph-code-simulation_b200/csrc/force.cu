@@ -221,6 +221,7 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
     const double dt = *dtp;
     const double gamma = P.gamma;
     unsigned long long solves = 0, iters = 0, fallbacks = 0;
+    unsigned n_cand = 0, n_pairs = 0;  // work counters of this lane
 
     for(long long wb = warp * GPW; wb < n; wb += nwarps * GPW) {
         const int i = (int)(wb + ((threadIdx.x & 31) / G));
@@ -250,6 +251,7 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
         const T mu_inv = T(1) / (mi * ui);
         const T r2i = T(1) / (rhoi * rhoi);
         double ax = 0, ay = 0, az = 0, de = 0;
+        n_cand += lane < cnt ? (unsigned)((cnt - lane + G - 1) / G) : 0u;
         for(int k = lane; k < cnt; k += G) {
             float yq = 0.f;
             int kk = k;
@@ -265,6 +267,7 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
             const double4 vj = S.vel[j];
             const double hj = vj.w;
             if(r >= (hi < hj ? hj : hi) || r == 0.0) continue;
+            ++n_pairs;
             const double4 tj = S.thermo[j];
             const T rT = (T)r;
             const T rinvT = (T)(1.0 / r);
@@ -467,6 +470,10 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
         } else if(valid && lane == 0) {
             S.acc[i] = make_double4(ax, ay, az, de);
         }
+    }
+    if(MODE != 4) {  // the completion pass re-solves pairs the force pass counted
+        block_count(&st->force_cand, n_cand);
+        block_count(&st->force_pairs, n_pairs);
     }
     if(TYPE == SPHGPU_GSPH) {
         for(int o = 16; o > 0; o >>= 1) {
@@ -698,14 +705,15 @@ int sphgpu_riemann_batch(sphgpu_ctx* c, const double* states, int64_t n, int mod
     double *d_st = nullptr, *d_p = nullptr, *d_v = nullptr;
     int *d_it = nullptr, *d_fb = nullptr;
     float* d_y = nullptr;
-    SPHGPU_CUDA(c, cudaMalloc(&d_st, sizeof(double) * 7 * (size_t)n));
+    DevTemps tmp(c->stream);
+    SPHGPU_CUDA(c, tmp.get(&d_st, sizeof(double) * 7 * (size_t)n, false));
     SPHGPU_CUDA(c, cudaMemcpyAsync(d_st, states, sizeof(double) * 7 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
-    SPHGPU_CUDA(c, cudaMalloc(&d_p, sizeof(double) * (size_t)n));
-    SPHGPU_CUDA(c, cudaMalloc(&d_v, sizeof(double) * (size_t)n));
-    SPHGPU_CUDA(c, cudaMalloc(&d_it, sizeof(int) * (size_t)n));
-    SPHGPU_CUDA(c, cudaMalloc(&d_fb, sizeof(int) * (size_t)n));
+    SPHGPU_CUDA(c, tmp.get(&d_p, sizeof(double) * (size_t)n, false));
+    SPHGPU_CUDA(c, tmp.get(&d_v, sizeof(double) * (size_t)n, false));
+    SPHGPU_CUDA(c, tmp.get(&d_it, sizeof(int) * (size_t)n, false));
+    SPHGPU_CUDA(c, tmp.get(&d_fb, sizeof(int) * (size_t)n, false));
     if(mode == 1) {
-        SPHGPU_CUDA(c, cudaMalloc(&d_y, sizeof(float) * (size_t)n));
+        SPHGPU_CUDA(c, tmp.get(&d_y, sizeof(float) * (size_t)n, false));
         const int rc = mlp_predict_states(c, d_st, n, d_y);
         if(rc < 0) return rc;
     }
@@ -717,12 +725,6 @@ int sphgpu_riemann_batch(sphgpu_ctx* c, const double* states, int64_t n, int mod
     if(vstar) SPHGPU_CUDA(c, cudaMemcpy(vstar, d_v, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost));
     if(iters) SPHGPU_CUDA(c, cudaMemcpy(iters, d_it, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost));
     if(fallbacks) SPHGPU_CUDA(c, cudaMemcpy(fallbacks, d_fb, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost));
-    cudaFree(d_st);
-    cudaFree(d_p);
-    cudaFree(d_v);
-    cudaFree(d_it);
-    cudaFree(d_fb);
-    if(d_y) cudaFree(d_y);
     return SPHGPU_OK;
 }
 

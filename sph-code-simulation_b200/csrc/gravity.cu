@@ -50,9 +50,10 @@ __global__ void __launch_bounds__(GBLK) k_gravity(DevParams P, DevState S, DevTr
     // node edges halve exactly per level: edge(L) = root edge * 2^(1 - L)
     const double root_edge = ldg4(&Tr.geo[0]).w;
     int nd = valid ? 0 : nnodes, steps = 0;
+    unsigned n_mono = 0, n_leaf = 0;  // work counters of this lane (steps = nodes met)
     while(nd < nnodes) {
         if(++steps > nnodes) {  // corrupt node table: report, never loop
-            st->guard = 1;
+            atomicOr(&st->pass_guard, PASS_GUARD_GRAVITY);
             break;
         }
         const int4 lk = __ldg(&Tr.link[nd]);
@@ -66,6 +67,7 @@ __global__ void __launch_bounds__(GBLK) k_gravity(DevParams P, DevState S, DevTr
             const double d2 = d.x * d.x + d.y * d.y + d.z * d.z;
             open = (l2 > P.theta2 * d2) || (d2 < l2);
             if(!open) {
+                ++n_mono;
                 const double rinv = 1.0 / sqrt(d2);
                 phi -= G * mc.w * rinv;
                 const double s = G * mc.w * (rinv * rinv * rinv);
@@ -74,6 +76,7 @@ __global__ void __launch_bounds__(GBLK) k_gravity(DevParams P, DevState S, DevTr
                 az -= d.z * s;
             }
             if(open && leaf) {
+                n_leaf += (unsigned)(lk.y - lk.x) - ((i >= lk.x && i < lk.y) ? 1u : 0u);
                 for(int q = lk.x; q < lk.y; ++q) {
                     if(q == i) continue;
                     const double4 pq = ldg4(&S.pos[q]);
@@ -94,6 +97,9 @@ __global__ void __launch_bounds__(GBLK) k_gravity(DevParams P, DevState S, DevTr
         S.acc[i] = make_double4(ax, ay, az, acc.w);
         S.visc[i].w = phi;
     }
+    block_count(&st->grav_nodes, (unsigned)min(steps, nnodes));
+    block_count(&st->grav_mono, n_mono);
+    block_count(&st->grav_leaf_pairs, n_leaf);
 }
 
 // -DEXHAUSTIVE_SEARCH direct summation (src/gravity_force.cpp:70-84): every j

@@ -134,9 +134,10 @@ __global__ void __launch_bounds__(MBLK, 8) k_gravity_mixed(DevParams P, DevState
     int since = 0;
     const int nnodes = *Tr.nnodes;
     int nd = valid ? 0 : nnodes, steps = 0;
+    unsigned n_mono = 0, n_leaf = 0;  // work counters of this lane (steps = nodes met)
     while(nd < nnodes) {
         if(++steps > nnodes) {  // corrupt node table: report, never loop
-            st->guard = 1;
+            atomicOr(&st->pass_guard, PASS_GUARD_GRAVITY32);
             break;
         }
         const float4 a = __ldg(&rec[nd].a);
@@ -154,6 +155,7 @@ __global__ void __launch_bounds__(MBLK, 8) k_gravity_mixed(DevParams P, DevState
         const float d2 = dx * dx + dy * dy + dz * dz;
         const bool open = (l2 > theta2 * d2) || (d2 < l2);
         if(!open) {
+            ++n_mono;
             const float rinv = rsqrtf(d2);
             const float gr = a.w * rinv;
             const float s = gr * rinv * rinv;
@@ -163,6 +165,7 @@ __global__ void __launch_bounds__(MBLK, 8) k_gravity_mixed(DevParams P, DevState
             fz -= dz * s;
         } else if(leaf) {
             const int4 lk = __ldg(&Tr.link[nd]);
+            n_leaf += (unsigned)(lk.y - lk.x) - ((i >= lk.x && i < lk.y) ? 1u : 0u);
             for(int q = lk.x; q < lk.y; ++q) {
                 if(q == i) continue;
                 const double4 pq = ldg4(&S.pos[q]);
@@ -197,6 +200,9 @@ __global__ void __launch_bounds__(MBLK, 8) k_gravity_mixed(DevParams P, DevState
         S.acc[i] = make_double4(ax + (double)fx, ay + (double)fy, az + (double)fz, acc.w);
         S.visc[i].w = phi + (double)fp;
     }
+    block_count(&st->grav_nodes, (unsigned)min(steps, nnodes));
+    block_count(&st->grav_mono, n_mono);
+    block_count(&st->grav_leaf_pairs, n_leaf);
 }
 
 }  // namespace

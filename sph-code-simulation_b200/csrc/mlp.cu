@@ -496,14 +496,14 @@ int mlp_infer_rows(sphgpu_ctx* c, const uint4* feat, float* y, long long rows)
 int mlp_predict_states(sphgpu_ctx* c, const double* d_states, long long n, float* d_y)
 {
     uint4* feat = nullptr;
-    SPHGPU_CUDA(c, cudaMalloc(&feat, sizeof(uint4) * (size_t)n));
+    DevTemps tmp(c->stream);
+    SPHGPU_CUDA(c, tmp.get(&feat, sizeof(uint4) * (size_t)n, false));
     k_state_features<<<grid_for(n, 256), 256, 0, c->stream>>>(d_states, nullptr, n, feat, nullptr);
     const long long tiles = (n + 15) / 16;
     const long long blocks = std::min<long long>((tiles + 3) / 4, 148LL * 16);
     k_mlp_infer<<<(unsigned)std::max<long long>(blocks, 1), IBLK, 0, c->stream>>>(mlp_device(c), feat, d_y, n);
     SPHGPU_LAUNCH_CHECK(c, "MLP predict");
     SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
-    cudaFree(feat);
     return SPHGPU_OK;
 }
 
@@ -528,25 +528,25 @@ static int upload_master(sphgpu_ctx* c)
     return SPHGPU_OK;
 }
 
-// device features/targets for host states; returns device buffers (caller frees)
-static int stage_states(sphgpu_ctx* c, const double* states, const double* pstar, int64_t n, uint4** feat,
-                        float** target)
+// device features/targets for host states, in buffers taken from `keep`
+// (released with it by the caller's scope)
+static int stage_states(sphgpu_ctx* c, DevTemps& keep, const double* states, const double* pstar, int64_t n,
+                        uint4** feat, float** target)
 {
     double *d_st = nullptr, *d_ps = nullptr;
-    SPHGPU_CUDA(c, cudaMalloc(&d_st, sizeof(double) * 7 * (size_t)n));
+    DevTemps tmp(c->stream);
+    SPHGPU_CUDA(c, tmp.get(&d_st, sizeof(double) * 7 * (size_t)n, false));
     SPHGPU_CUDA(c, cudaMemcpyAsync(d_st, states, sizeof(double) * 7 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
     if(pstar) {
-        SPHGPU_CUDA(c, cudaMalloc(&d_ps, sizeof(double) * (size_t)n));
+        SPHGPU_CUDA(c, tmp.get(&d_ps, sizeof(double) * (size_t)n, false));
         SPHGPU_CUDA(c, cudaMemcpyAsync(d_ps, pstar, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
     }
-    SPHGPU_CUDA(c, cudaMalloc(feat, sizeof(uint4) * (size_t)n));
+    SPHGPU_CUDA(c, keep.get(feat, sizeof(uint4) * (size_t)n, false));
     *target = nullptr;
-    if(pstar) SPHGPU_CUDA(c, cudaMalloc(target, sizeof(float) * (size_t)n));
+    if(pstar) SPHGPU_CUDA(c, keep.get(target, sizeof(float) * (size_t)n, false));
     k_state_features<<<grid_for(n, 256), 256, 0, c->stream>>>(d_st, d_ps, n, *feat, *target);
     SPHGPU_LAUNCH_CHECK(c, "MLP features");
     SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
-    cudaFree(d_st);
-    if(d_ps) cudaFree(d_ps);
     return SPHGPU_OK;
 }
 
@@ -605,18 +605,17 @@ int sphgpu_mlp_predict(sphgpu_ctx* c, const double* states, int64_t n, float* y)
     if(!c->have_mlp) return fail(c, SPHGPU_ERR_NO_MLP, "no MLP parameters loaded");
     uint4* feat = nullptr;
     float* tgt = nullptr;
-    int rc = stage_states(c, states, nullptr, n, &feat, &tgt);
+    DevTemps tmp(c->stream);
+    int rc = stage_states(c, tmp, states, nullptr, n, &feat, &tgt);
     if(rc) return rc;
     float* d_y = nullptr;
-    SPHGPU_CUDA(c, cudaMalloc(&d_y, sizeof(float) * (size_t)n));
+    SPHGPU_CUDA(c, tmp.get(&d_y, sizeof(float) * (size_t)n, false));
     const long long tiles = (n + 15) / 16;
     const long long blocks = std::min<long long>((tiles + 3) / 4, 148LL * 16);
     k_mlp_infer<<<(unsigned)blocks, IBLK, 0, c->stream>>>(mlp_device(c), feat, d_y, n);
     SPHGPU_LAUNCH_CHECK(c, "MLP predict");
     SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));  // the context stream does not sync with cudaMemcpy
     SPHGPU_CUDA(c, cudaMemcpy(y, d_y, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost));
-    cudaFree(d_y);
-    cudaFree(feat);
     return SPHGPU_OK;
 }
 
@@ -634,12 +633,13 @@ int sphgpu_mlp_train(sphgpu_ctx* c, const double* states, const double* pstar, i
     }
     uint4* feat = nullptr;
     float* tgt = nullptr;
-    int rc = stage_states(c, states, pstar, n, &feat, &tgt);
+    DevTemps tmp(c->stream);
+    int rc = stage_states(c, tmp, states, pstar, n, &feat, &tgt);
     if(rc) return rc;
     float *grad = nullptr, *m1 = c->d_mlp_master + MLP_NPARAM, *m2 = c->d_mlp_master + 2 * MLP_NPARAM;
     float* d_loss = nullptr;
-    SPHGPU_CUDA(c, cudaMalloc(&grad, sizeof(float) * MLP_NPARAM));
-    SPHGPU_CUDA(c, cudaMalloc(&d_loss, sizeof(float)));
+    SPHGPU_CUDA(c, tmp.get(&grad, sizeof(float) * MLP_NPARAM, false));
+    SPHGPU_CUDA(c, tmp.get(&d_loss, sizeof(float), false));
     SPHGPU_CUDA(c, cudaMemsetAsync(m1, 0, sizeof(float) * 2 * MLP_NPARAM, c->stream));
     MlpDev md = mlp_device(c);
     const __nv_bfloat16* wt1 = md.w + IMG_W1T;
@@ -706,10 +706,6 @@ int sphgpu_mlp_train(sphgpu_ctx* c, const double* states, const double* pstar, i
     c->mlp_master.resize(MLP_NPARAM);
     SPHGPU_CUDA(c, cudaMemcpy(c->mlp_master.data(), c->d_mlp_master, sizeof(float) * MLP_NPARAM,
                               cudaMemcpyDeviceToHost));
-    cudaFree(grad);
-    cudaFree(d_loss);
-    cudaFree(feat);
-    cudaFree(tgt);
     return SPHGPU_OK;
 }
 

@@ -81,6 +81,7 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
     const bool av_energy = disph && !(gdisph && P.balsara);
     double hv_min = DBL_MAX;
     unsigned nonconv = 0;
+    unsigned n_cand = 0, n_newton = 0, n_pairs = 0;  // work counters of this lane
 
     for(long long wb = warp * GPW; wb < n; wb += nwarps * GPW) {
         const int i = (int)(wb + ((threadIdx.x & 31) / G));
@@ -106,6 +107,7 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
                 // the next candidate's index is fetched one iteration ahead,
                 // so the position load does not wait on the list load
                 int jn = lane < cnt ? __ldg(&li[lane]) : 0;
+                n_cand += lane < cnt ? (unsigned)((cnt - lane + G - 1) / G) : 0u;
                 for(int k = lane; k < cnt; k += G) {
                     const int jc = jn;
                     if(k + G < cnt) jn = __ldg(&li[k + G]);
@@ -113,6 +115,7 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
                     Vec3d dv;
                     const double r = r_within(P, pi.x, pi.y, pi.z, pj, h, dv);
                     if(r >= 0.0 && r < h) {
+                        ++n_newton;
                         const T w = kh.w((T)r);
                         const T dh = kh.dhw((T)r);
                         if(disph) {
@@ -150,6 +153,7 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
         const bool need_av = !gsph && (P.balsara || P.td_av);
         const bool need_grad = (gsph || gdisph) && P.gsph2;
         int jn2 = lane < cnt ? __ldg(&li[lane]) : 0;
+        n_cand += lane < cnt ? (unsigned)((cnt - lane + G - 1) / G) : 0u;
         for(int k = lane; k < cnt; k += G) {
             const int j = jn2;
             if(k + G < cnt) jn2 = __ldg(&li[k + G]);
@@ -217,6 +221,7 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
                 }
             }
         }
+        n_pairs += (unsigned)nn;
         const double densS = (double)group_sum<G>(dens);
         nn = group_sum<G>(nn);
         vsig = group_max<G>(vsig);
@@ -340,6 +345,9 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
         if(m < DBL_MAX) atomic_min_pos(hvs, m);
         if(c) atomicAdd(&st->newton_nonconv, (unsigned long long)c);
     }
+    block_count(&st->pre_cand, n_cand);
+    block_count(&st->pre_newton_pairs, n_newton);
+    block_count(&st->pre_pairs, n_pairs);
 }
 
 // PreInteraction::initial_smoothing (src/pre_interaction.cpp:171-215):

@@ -30,6 +30,7 @@
 // -fmad=false), so node geometry, mass and centre of mass are bit-identical
 // to the reference's.
 #include <cfloat>
+#include <cstddef>
 #include <cuda_runtime.h>
 
 #include "context.cuh"
@@ -407,7 +408,7 @@ __global__ void k_mass_up(int n, const int* __restrict__ leaf_of_start, DevTree 
     // at most 22 levels up, at most 8 children per node: bounded loops
     for(int up = 0; node != 0; ++up) {
         if(up > 64) {
-            st->guard = 1;
+            atomicOr(&st->pass_guard, PASS_GUARD_MASS);
             return;
         }
         const int par = T.parent[node];
@@ -457,7 +458,7 @@ __global__ void k_ksize_up(int n, const int* __restrict__ leaf_of_start, DevTree
     }
     for(int up = 0; node != 0; ++up) {
         if(up > 64) {
-            st->guard = 1;
+            atomicOr(&st->pass_guard, PASS_GUARD_KSIZE);
             return;
         }
         const int par = T.parent[node];
@@ -490,7 +491,11 @@ int tree_make(sphgpu_ctx* c)
     // root cube
     const int nb = (int)std::min<long long>(grid_for(n, BLK), 1024);
     int launches = 3;  // root, keys, levels
-    SPHGPU_CUDA(c, cudaMemsetAsync(&c->d_status->nonfinite, 0, sizeof(int), st));
+    // node_pool, guard and nonfinite are adjacent words: clear all three, so an
+    // earlier "no free node" does not outlive a new upload
+    static_assert(offsetof(DevStatus, nonfinite) == offsetof(DevStatus, node_pool) + 2 * sizeof(int),
+                  "status word layout");
+    SPHGPU_CUDA(c, cudaMemsetAsync(&c->d_status->node_pool, 0, 3 * sizeof(int), st));
     k_bbox_partial<<<nb, BLK, 0, st>>>(c->s.pos, n, c->d_bbox_part, c->d_status);
     ++launches;
     k_root<<<1, 32, 0, st>>>(c->d_bbox_part, nb, c->dp, c->d_root);
@@ -509,6 +514,14 @@ int tree_make(sphgpu_ctx* c)
     int nnodes = 0;
     SPHGPU_CUDA(c, cudaMemcpyAsync(&nnodes, c->t.nnodes, sizeof(int), cudaMemcpyDeviceToHost, st));
     SPHGPU_CUDA(c, cudaStreamSynchronize(st));
+    {
+        // a bound hit by set_kernel or gravity since the last wait
+        const int rcg = check_pass_guard(c);
+        if(rcg < 0) {
+            c->have_tree = false;
+            return rcg;
+        }
+    }
     if(c->h_status.nonfinite) {
         c->have_tree = false;
         return fail(c, SPHGPU_ERR_STATE, "non-finite particle position");

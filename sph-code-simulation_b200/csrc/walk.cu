@@ -33,6 +33,7 @@
 // longer than the capacity is counted but not stored; the host grows the
 // buffer and re-runs (status.overflow).  More than neighbor_number * 1000
 // entries is the reference's fatal overflow (src/bhtree.cpp:129-135).
+#include <cstddef>
 #include <cuda_runtime.h>
 
 #include "context.cuh"
@@ -596,11 +597,18 @@ int run_walk(sphgpu_ctx* c, int which, bool guess, double ratio, bool exhaustive
                                                            c->d_status, 0, 1.0);
         }
         SPHGPU_LAUNCH_CHECK(c, "neighbour walk");
-        SPHGPU_CUDA(c, cudaMemcpyAsync(&c->h_status, c->d_status, 5 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        // the first seven status words: the walk's own and the pass guard of
+        // the bottom-up mass pass that ran before it
+        static_assert(offsetof(DevStatus, pass_guard) == 6 * sizeof(int), "status word layout");
+        SPHGPU_CUDA(c, cudaMemcpyAsync(&c->h_status, c->d_status, 7 * sizeof(int), cudaMemcpyDeviceToHost, st));
         SPHGPU_CUDA(c, cudaStreamSynchronize(st));
         if(c->h_status.fatal) {
             return fail(c, SPHGPU_ERR_NEIGHBOR_OVERFLOW,
                         "Neighbor list overflow: more than neighborNumber * 1000 neighbours");
+        }
+        {
+            const int rcg = check_pass_guard(c);
+            if(rcg < 0) return rcg;
         }
         if(c->h_status.guard == 2 && !per_lane) {
             // a warp's traversal stack overflowed: redo this call with the per-lane walk
@@ -655,7 +663,8 @@ int export_lists(sphgpu_ctx* c, int which, int64_t* offsets, int32_t* ids, int64
     const int* list = which == 0 ? c->d_glist : c->d_plist;
     const int* count = which == 0 ? c->d_gcount : c->d_pcount;
     unsigned long long *d_cnt = nullptr, *d_off = nullptr, *d_tot = nullptr;
-    SPHGPU_CUDA(c, cudaMallocAsync(&d_cnt, sizeof(unsigned long long) * (size_t)(2 * n + 2), st));
+    DevTemps tmp(st);
+    SPHGPU_CUDA(c, tmp.get(&d_cnt, sizeof(unsigned long long) * (size_t)(2 * n + 2)));
     d_off = d_cnt + n;
     d_tot = d_off + n;
     k_counts_by_id<<<grid_for(n, 256), 256, 0, st>>>(n, c->s.id, count, d_cnt);
@@ -674,13 +683,11 @@ int export_lists(sphgpu_ctx* c, int which, int64_t* offsets, int32_t* ids, int64
             rc = fail(c, SPHGPU_ERR_ARG, "neighbour id buffer too small");
         } else {
             int* d_ids = nullptr;
-            SPHGPU_CUDA(c, cudaMallocAsync(&d_ids, sizeof(int) * (size_t)(total + 1), st));
+            SPHGPU_CUDA(c, tmp.get(&d_ids, sizeof(int) * (size_t)(total + 1)));
             k_fill_by_id<<<grid_for(n, 256), 256, 0, st>>>(n, (int)lcap, c->s.id, count, list, d_off, d_ids);
             SPHGPU_CUDA(c, cudaMemcpyAsync(ids, d_ids, sizeof(int) * (size_t)total, cudaMemcpyDeviceToHost, st));
-            SPHGPU_CUDA(c, cudaFreeAsync(d_ids, st));
         }
     }
-    SPHGPU_CUDA(c, cudaFreeAsync(d_cnt, st));
     SPHGPU_CUDA(c, cudaStreamSynchronize(st));
     return rc;
 }

@@ -72,3 +72,43 @@ def test_calls_out_of_order_are_rejected(gpu):
         sim.upload(_cube(6, 0.3))
         with pytest.raises(gpu.SPHException, match="before tree"):
             sim.fluid_force()
+
+
+def test_node_pool_error_does_not_outlive_a_new_upload(gpu):
+    """Two particles closer than the deepest level can split need a chain of
+    more nodes than the 5 N + 2 pool holds: the reference's "There is no free
+    node." (src/bhtree.cpp:222-224).  A later valid upload of the same size
+    builds its tree."""
+    f = {"pos_x": np.array([0.5, 0.5 + 1e-9]), "pos_y": np.full(2, 0.5), "pos_z": np.full(2, 0.5),
+         "mass": np.full(2, 0.5), "dens": np.ones(2), "ene": np.ones(2), "sml": np.full(2, 0.1)}
+    with gpu.Simulation(gpu.default_params()) as sim:
+        sim.upload(f)
+        with pytest.raises(gpu.SPHException, match="no free node"):
+            sim.tree_make()
+        f["pos_x"][1] = -0.5
+        sim.upload(f)
+        sim.tree_make()
+        assert sim.counters()["node_count"] >= 3
+
+
+@pytest.mark.parametrize("bits,what", [(1, "mass"), (2, "set_kernel"), (4, "gravity walk"),
+                                       (8, "mixed gravity walk")])
+def test_pass_guard_is_reported_at_the_next_wait(gpu, bits, what):
+    """The bottom-up passes and the gravity walks bound their loops and set a
+    status bit instead of looping on a corrupt tree; the bit is reported by
+    the next call that waits on the stream, and the context stays usable."""
+    p = gpu.config_params("evrard_ssph")
+    f = gpu.sample_evrard(8)
+    with gpu.Simulation(p) as sim:
+        sim.upload(f)
+        sim.initialize()
+        gpu.lib().sphgpu_test_flag_pass_guard(sim._h, bits)
+        with pytest.raises(gpu.SPHException, match=what):
+            sim.synchronize()
+        sim.synchronize()                      # reported once, then cleared
+        gpu.lib().sphgpu_test_flag_pass_guard(sim._h, bits)
+        with pytest.raises(gpu.SPHException, match="bounded device pass"):
+            sim.integrate()                    # tree_make's wait sees it
+        sim.upload(f)
+        sim.initialize()
+        sim.integrate()
