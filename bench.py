@@ -656,7 +656,8 @@ def _cpu_reference(steps: int, warmup: int, workload: str, n_target, budget_s: f
             break
     return {"value": n * done / el, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": kind,
             "ms_per_step": 1e3 * el / done, "steps": done, "n": n,
-            "sample": f"N={n} (the full workload), initialize ({t_init:.1f} s, untimed) + {warmup} untimed + "
+            "sample": f"N={n}{' (the full workload)' if n >= wl.default_n * 0.99 else ' (a smaller lattice of the same workload)'}, "
+                      f"initialize ({t_init:.1f} s, untimed) + {warmup} untimed + "
                       f"{done} timed steps ({el:.1f} s); host {_cpu_model()}"}
 
 
@@ -674,7 +675,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--verbose", action="store_true")
-    ap.add_argument("--ref-budget", type=float, default=240.0,
+    ap.add_argument("--ref-budget", type=float, default=150.0,
                     help="reference arm: wall seconds of timed CPU steps before it stops (at least one step)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

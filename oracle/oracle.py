@@ -23,6 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libsphref.so")
 REF_EXH_LIB = os.path.join(HERE, "_ref", "libsphref_exh.so")
+REF_GPU_LIB = os.path.join(HERE, "_ref", "libsphref_gpu.so")
 
 # the field order of include/sphgpu.h
 FIELDS = [
@@ -39,10 +40,16 @@ NF = len(FIELDS)
 FI = {f: k for k, f in enumerate(FIELDS)}
 
 
+def refdir() -> str:
+    """The reference checkout: $REFDIR, else a "reference" directory beside
+    the repository (the Makefile's default)."""
+    return os.environ.get("REFDIR") or os.path.normpath(os.path.join(HERE, os.pardir, os.pardir, "reference"))
+
+
 def build(reference: bool = True) -> None:
     """make -C oracle (the reference part only when its sources are present)."""
     targets = ["oracle"]
-    if reference and os.path.isdir(os.environ.get("REFDIR", "/root/reference")):
+    if reference and os.path.isdir(refdir()):
         targets.append("ref")
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
@@ -99,6 +106,8 @@ def _load(path: str, prefix: str) -> C.CDLL:
         L.ref_energies.argtypes = [vp, dp, dp, dp]
         L.ref_module_times.argtypes = [vp, dp]
         L.ref_relax_step.argtypes = [vp, C.c_char_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, dp]
+        L.ref_set_swap_mode.restype = C.c_int
+        L.ref_set_swap_mode.argtypes = [C.c_int]
     for name in ("destroy", "get", "set", "tree_make", "set_kernel", "pre", "force", "timestep", "predict",
                  "correct", "initialize", "integrate", "neighbor_lists", "get_dt", "set_dt", "get_time",
                  "get_h_per_v_sig", "last_error"):
@@ -293,6 +302,26 @@ class Reference(_Base):
         out = (C.c_double * 7)()
         self.L.ref_module_times(self.h, C.cast(out, C.POINTER(C.c_double)))
         return list(out)
+
+
+class ReferenceWithGpuModules(Reference):
+    """The reference's Solver sequence (oracle/ref_harness.cpp) with the GPU
+    modules of sph-code-simulation_b200/host/gpu_modules.hpp swapped in for
+    TimeStep, PreInteraction, FluidForce, GravityForce and make_tree
+    (oracle/_ref/libsphref_gpu.so).  resident=False keeps Solver::predict /
+    correct on the host (MIRROR), True runs them on the device (RESIDENT)."""
+
+    def __init__(self, params, fields: Dict[str, np.ndarray], resident: bool = False, threads: int = 0):
+        self.L = _load(REF_GPU_LIB, "ref")
+        if threads <= 0:
+            threads = int(os.environ.get("OMP_NUM_THREADS", "0") or 0) or max(2, os.cpu_count() or 2)
+        self.L.ref_set_threads(threads)
+        self.L.ref_set_swap_mode(int(resident))
+        self.n = len(fields["pos_x"])
+        ptrs, keep = _ptrs(fields, self.n)
+        self.h = self.L.ref_create(C.byref(params), self.n, ptrs)
+        if not self.h:
+            raise RuntimeError("ref_create failed")
 
 
 def kernel_w(kind: int, r: float, h: float) -> float:

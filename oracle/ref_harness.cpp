@@ -48,6 +48,12 @@
 #include <unistd.h>
 
 #include "sphgpu.h"
+#ifdef SPHGPU_SWAP
+// libsphref_gpu.so: the same Solver sequence with the GPU modules of
+// sph-code-simulation_b200/host/gpu_modules.hpp swapped in for TimeStep,
+// PreInteraction, FluidForce, GravityForce and Simulation::make_tree
+#include "gpu_modules.hpp"
+#endif
 
 using namespace sph;
 
@@ -60,7 +66,18 @@ struct RefCtx {
     std::shared_ptr<LaneEmdenRelaxation> relax;
     std::string err;
     double t_module[8] = {0};  // seconds: timestep, predict, tree, pre, force, gravity, correct, total
+#ifdef SPHGPU_SWAP
+    std::shared_ptr<GpuContext> gpu;
+#endif
 };
+
+#ifdef SPHGPU_SWAP
+int g_swap_resident = 0;  // 0: MIRROR (host predict / correct), 1: RESIDENT
+
+void make_tree(RefCtx& c) { c.gpu->make_tree(*c.sim); }
+#else
+void make_tree(RefCtx& c) { c.sim->make_tree(); }
+#endif
 
 std::shared_ptr<SPHParameters> to_param(const sphgpu_params* p)
 {
@@ -207,6 +224,34 @@ void correct(RefCtx& c)
     }
 }
 
+// Solver::predict / correct as the swapped-in binding runs them: on the host
+// (MIRROR) or on the device (RESIDENT).
+void step_predict(RefCtx& c)
+{
+#ifdef SPHGPU_SWAP
+    if(g_swap_resident) return c.gpu->predict(*c.sim);
+#endif
+    predict(c);
+}
+
+void step_correct(RefCtx& c)
+{
+#ifdef SPHGPU_SWAP
+    if(g_swap_resident) return c.gpu->correct(*c.sim);
+#endif
+    correct(c);
+}
+
+// The host particles are current (RESIDENT keeps them on the device).
+void host_current(RefCtx& c)
+{
+#ifdef SPHGPU_SWAP
+    if(g_swap_resident) c.gpu->to_host(*c.sim);
+#else
+    (void)c;
+#endif
+}
+
 template <typename F>
 int guarded(RefCtx* c, F&& f)
 {
@@ -318,6 +363,18 @@ void* ref_create(const sphgpu_params* p, int64_t n, const double* const* fields)
         c->fforce = std::make_shared<FluidForce>();
     }
     c->gforce = std::make_shared<GravityForce>();
+#ifdef SPHGPU_SWAP
+    try {
+        c->gpu = std::make_shared<GpuContext>(*c->param, g_swap_resident ? GpuContext::RESIDENT : GpuContext::MIRROR);
+    } catch(SPHException&) {  // no usable device
+        delete c;
+        return nullptr;
+    }
+    c->timestep = std::make_shared<GpuTimeStep>(c->gpu);
+    c->pre = std::make_shared<GpuPreInteraction>(c->gpu);
+    c->fforce = std::make_shared<GpuFluidForce>(c->gpu);
+    c->gforce = std::make_shared<GpuGravityForce>(c->gpu);
+#endif
     c->timestep->initialize(c->param);
     c->pre->initialize(c->param);
     c->fforce->initialize(c->param);
@@ -332,6 +389,18 @@ void ref_destroy(void* h) { delete static_cast<RefCtx*>(h); }
 // (more than one thread: the box also covers the origin), and the SRGSPH
 // context sets it to 1 for the whole process.
 void ref_set_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }
+// libsphref_gpu.so: how the swapped-in GPU modules keep the particles
+// (0 = MIRROR, 1 = RESIDENT); returns -1 in the CPU-only builds.
+int ref_set_swap_mode(int resident)
+{
+#ifdef SPHGPU_SWAP
+    g_swap_resident = resident ? 1 : 0;
+    return 0;
+#else
+    (void)resident;
+    return -1;
+#endif
+}
 int ref_max_threads(void) { return omp_get_max_threads(); }
 
 const char* ref_last_error(void* h) { return static_cast<RefCtx*>(h)->err.c_str(); }
@@ -440,12 +509,12 @@ int ref_initialize(void* h)
             p[i].sound = std::sqrt(c_sound * p[i].ene);
         }
 #ifndef EXHAUSTIVE_SEARCH
-        auto tree = c->sim->get_tree();
-        tree->make(p, num);
+        make_tree(*c);
 #endif
         c->pre->calculation(c->sim);
         c->fforce->calculation(c->sim);
         c->gforce->calculation(c->sim);
+        host_current(*c);
     });
 }
 
@@ -458,10 +527,10 @@ int ref_integrate(void* h)
         double t0 = now(), t1;
         c->timestep->calculation(c->sim);
         t1 = now(); c->t_module[0] += t1 - t0; t0 = t1;
-        predict(*c);
+        step_predict(*c);
         t1 = now(); c->t_module[1] += t1 - t0; t0 = t1;
 #ifndef EXHAUSTIVE_SEARCH
-        c->sim->make_tree();
+        make_tree(*c);
 #endif
         t1 = now(); c->t_module[2] += t1 - t0; t0 = t1;
         c->pre->calculation(c->sim);
@@ -470,7 +539,8 @@ int ref_integrate(void* h)
         t1 = now(); c->t_module[4] += t1 - t0; t0 = t1;
         c->gforce->calculation(c->sim);
         t1 = now(); c->t_module[5] += t1 - t0; t0 = t1;
-        correct(*c);
+        step_correct(*c);
+        host_current(*c);
         t1 = now(); c->t_module[6] += t1 - t0;
         c->sim->update_time();
     });

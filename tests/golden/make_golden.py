@@ -1,7 +1,8 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
 Run in a container where the reference sources are mounted (default
-/root/reference, override with REFDIR) after `make -C oracle`:
+a "reference" directory beside the repository, override with REFDIR) after
+`make -C oracle`:
 
     python tests/golden/make_golden.py
 
@@ -84,7 +85,8 @@ import oracle as O  # noqa: E402
 import sphgpu as G  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
-REFDIR = os.environ.get("REFDIR", "/root/reference")
+# the reference checkout: REFDIR, else a "reference" directory beside the repository
+REFDIR = os.environ.get("REFDIR") or os.path.normpath(os.path.join(ROOT, os.pardir, "reference"))
 
 STATE_FIELDS = ["pos_x", "pos_y", "pos_z", "vel_x", "vel_y", "vel_z", "acc_x", "acc_y", "acc_z", "mass",
                 "dens", "pres", "ene", "dene", "sml", "sound", "balsara", "alpha", "gradh", "phi", "neighbor",

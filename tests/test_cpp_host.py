@@ -7,6 +7,8 @@ import pytest
 
 from conftest import PKG, ROOT
 
+import oracle  # noqa: E402  (conftest puts oracle/ on sys.path)
+
 
 def _build(tmp_path):
     exe = tmp_path / "host_mirror"
@@ -34,26 +36,19 @@ def test_host_mirror_runs_steps(gpu, tmp_path):
 
 
 def test_reference_side_binding_compiles(tmp_path):
-    """The Module subclasses of the integration guide (its C++ block, what a
-    maintainer adds beside src/solver.cpp) compile against the reference's
-    own headers (include/module.hpp, simulation.hpp,
-    parameters.hpp, exception.hpp) and include/sphgpu.h, with the flags the
-    reference's sources build with."""
-    refdir = os.environ.get("REFDIR", "/root/reference")
+    """The reference-side binding (host/gpu_modules.hpp: the four GPU Module
+    subclasses and the particle sync) compiles against the reference's own
+    headers (include/module.hpp, simulation.hpp, parameters.hpp, particle.hpp,
+    exception.hpp) and include/sphgpu.h, with the flags the reference's
+    sources build with."""
+    refdir = oracle.refdir()
     if not os.path.isdir(os.path.join(refdir, "include")):
         pytest.skip("the reference's headers are not mounted here")
-    lines, inside = [], False
-    for ln in open(os.path.join(ROOT, "INTEGRATION.md")):
-        if ln.startswith("```cpp"):
-            inside = True
-        elif ln.startswith("```"):
-            inside = False
-        elif inside:
-            lines.append(ln)
-    assert lines, "no C++ block in the integration guide"
-    src = tmp_path / "gpu_modules.cpp"
-    src.write_text("".join(lines))
+    src = tmp_path / "use_gpu_modules.cpp"
+    src.write_text('#include "gpu_modules.hpp"\n'
+                   "int main() { sph::SPHParameters p{}; (void)sph::GpuContext::params(p); return 0; }\n")
     r = subprocess.run(["g++", "-std=c++14", "-fsyntax-only", "-fopenmp", "-DDIM=3", "-include", "string",
                         "-include", "limits", "-I", os.path.join(refdir, "include"), "-I",
-                        os.path.join(ROOT, "include"), str(src)], capture_output=True, text=True)
+                        os.path.join(ROOT, "include"), "-I", os.path.join(PKG, "host"), str(src)],
+                       capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
