@@ -302,9 +302,10 @@ def run_gpu(args, rank: int, world: int, local: int):
     n = len(fields["pos_x"])
     hbm, peak_kind = _peaks()
 
-    def timed(precision):
-        log(f"{wl.name} n={n} precision={precision}: initialize")
+    def timed(precision, acc_tol=0.0):
+        log(f"{wl.name} n={n} precision={precision} mixed_acc_tol={acc_tol}: initialize")
         p = wl.params(precision)
+        p.mixed_acc_tol = acc_tol
         sim = G.Simulation(p)
         if wl.learned:
             sim.load_riemann_mlp()
@@ -365,6 +366,15 @@ def run_gpu(args, rank: int, world: int, local: int):
                  "dtype": "f32 pair/gravity, f64 accumulators and kick-drift",
                  "stages_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in mstages.items()}}
         msim.close()
+        # the same with the FP64 re-evaluation of particles whose FP32 force /
+        # gravity rounding could exceed 1e-5 of their acceleration
+        csim, _, cms, _, _, cstages, ccounters = timed(SP.MIXED, 1e-5)
+        cms_max = max_over_ranks(cms)
+        mixed["checked_1e-5"] = {
+            "value": whole_job_value(n * args.steps, world, cms_max), "ms_per_step": cms_max / args.steps,
+            "rechecked_fraction": ccounters["mixed_rechecks"] / float(n * args.steps),
+            "recheck_ms_per_step": round(cstages["recheck"][0] / args.steps, 4)}
+        csim.close()
 
     # FLOP rooflines of the arithmetic stages against measured GEMM peaks
     try:

@@ -114,6 +114,20 @@ typedef struct sphgpu_params {
     double  sr_c_cd;               /* "cContactDiscontinuity" (1.0)         */
     double  sr_eta;                /* "etaSmoothingLength" (1.0)            */
     double  sr_c_smooth;           /* "cSmoothGradient" (2.0)               */
+    /* Mixed form only (no counterpart in the reference): per-particle bound
+     * on the FP32 rounding error of the FluidForce and GravityForce sums,
+     * relative to the acceleration.  After GravityForce, particles whose
+     * error estimate (8 x 2^-24 x the sum of the absolute values of their
+     * FP32 force and gravity terms) exceeds it are re-evaluated in FP64
+     * (FluidForce and GravityForce on the same lists and tree).  It bounds
+     * the rounding of the force and gravity terms, not that of the FP32
+     * PreInteraction outputs (density, pressure) they read.  0 = off.  (0) */
+    double  mixed_acc_tol;
+    /* Relative change of p at which the plain iterative Riemann solver stops
+     * (src/gsph/g_fluid_force.cpp:262 stops at 1e-6; a smaller value runs
+     * the same Newton iteration further, for like-for-like comparisons with
+     * the learned start, which always refines to 1e-10).  (1e-6)          */
+    double  riemann_tol;
 } sphgpu_params;
 
 /* Per-particle fields, in the order of sph::SPHParticle where it has them
@@ -168,6 +182,9 @@ typedef struct sphgpu_counters {
     int64_t gravity_nodes;         /* tree nodes met (opening tests)         */
     int64_t gravity_monopoles;     /* nodes taken as monopoles               */
     int64_t gravity_leaf_pairs;    /* softened particle pairs                */
+    int64_t mixed_rechecks;        /* mixed form: particles whose FluidForce and
+                                      GravityForce were re-evaluated in FP64
+                                      (mixed_acc_tol)                       */
 } sphgpu_counters;
 
 /* Stage timers (ms, summed since the last reset; CUDA events on the
@@ -175,7 +192,9 @@ typedef struct sphgpu_counters {
 enum sphgpu_stage {
     SPHGPU_T_TIMESTEP = 0, SPHGPU_T_PREDICT, SPHGPU_T_TREE, SPHGPU_T_GATHER_WALK,
     SPHGPU_T_PRE, SPHGPU_T_SET_KERNEL, SPHGPU_T_PAIR_WALK, SPHGPU_T_FORCE,
-    SPHGPU_T_GRAVITY, SPHGPU_T_CORRECT, SPHGPU_NSTAGES
+    SPHGPU_T_GRAVITY, SPHGPU_T_CORRECT,
+    SPHGPU_T_RECHECK,   /* mixed form: FP64 re-evaluation (mixed_acc_tol) */
+    SPHGPU_NSTAGES
 };
 
 typedef struct sphgpu_ctx sphgpu_ctx;

@@ -27,7 +27,7 @@ NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-rela
            "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 EXACT = {"tree.cu", "walk.cu", "gravity.cu", "integrate.cu", "noalloc.cu", "relax.cu", "srgsph.cu"}
 SOURCES = ["scan_sort.cu", "tree.cu", "walk.cu", "pre.cu", "force.cu", "gravity.cu", "gravity_mixed.cu", "flist.cu",
-           "integrate.cu", "mlp.cu", "capi.cu", "noalloc.cu", "relax.cu", "srgsph.cu"]
+           "integrate.cu", "mlp.cu", "capi.cu", "noalloc.cu", "relax.cu", "srgsph.cu", "recheck.cu"]
 HOST_SOURCES = ["samples.cpp", "csv.cpp"]
 
 

@@ -127,6 +127,8 @@ void set_dev_params(sphgpu_ctx* c)
     d.sr_c_cd = p.sr_c_cd;
     d.sr_eta = p.sr_eta;
     d.sr_c_smooth = p.sr_c_smooth;
+    d.mixed_acc_tol = p.mixed_acc_tol;
+    d.riemann_tol = p.riemann_tol;
     d.av_alpha = p.av_alpha;
     d.balsara = p.use_balsara_switch;
     d.td_av = p.use_time_dependent_av;
@@ -423,6 +425,8 @@ int check_params(const sphgpu_params* p, std::string& why)
     }
     if(p->use_time_dependent_av && p->alpha_max < p->alpha_min) return why = "alphaMax < alphaMin", -1;
     if(p->precision != SPHGPU_FP64 && p->precision != SPHGPU_MIXED) return why = "precision must be fp64 or mixed", -1;
+    if(!(p->mixed_acc_tol >= 0.0)) return why = "mixed_acc_tol must be >= 0", -1;
+    if(!(p->riemann_tol > 0.0 && p->riemann_tol < 1.0)) return why = "riemann_tol must be in (0, 1)", -1;
     return 0;
 }
 
@@ -469,6 +473,8 @@ void sphgpu_default_params(sphgpu_params* p)
     p->sr_c_cd = 1.0;
     p->sr_eta = 1.0;
     p->sr_c_smooth = 2.0;
+    p->mixed_acc_tol = 0.0;
+    p->riemann_tol = 1e-6;
 }
 
 int sphgpu_device_ok(void)
@@ -516,6 +522,7 @@ int sphgpu_destroy(sphgpu_ctx* c)
     if(c->d_mlp_defer) cudaFree(c->d_mlp_defer);
     if(c->d_harvest) cudaFree(c->d_harvest);
     if(c->d_harvest_count) cudaFree(c->d_harvest_count);
+    if(c->d_recheck) cudaFree(c->d_recheck);
     stage_flush(c);
     for(cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     for(cudaEvent_t e : c->user_ev) {
@@ -913,6 +920,7 @@ int sphgpu_get_counters(sphgpu_ctx* c, sphgpu_counters* o)
     o->gravity_nodes = (int64_t)c->h_status.grav_nodes;
     o->gravity_monopoles = (int64_t)c->h_status.grav_mono;
     o->gravity_leaf_pairs = (int64_t)c->h_status.grav_leaf_pairs;
+    o->mixed_rechecks = c->mixed_rechecks;
     return SPHGPU_OK;
 }
 
@@ -925,6 +933,7 @@ int sphgpu_reset_counters(sphgpu_ctx* c)
     }
     std::memset(&c->h_status, 0, sizeof(c->h_status));
     c->retries = 0;
+    c->mixed_rechecks = 0;
     return SPHGPU_OK;
 }
 

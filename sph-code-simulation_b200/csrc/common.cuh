@@ -47,6 +47,8 @@ struct DevParams {
     double ratio;  // kernel ratio 1.2 (iterative sml) or 1.0 (src/pre_interaction.cpp:31-35)
     int sr_2nd;    // srgsph: MUSCL reconstruction
     double sr_c, sr_c_shock, sr_c_cd, sr_eta, sr_c_smooth;
+    double mixed_acc_tol;  // mixed form: FP64 re-evaluation above this estimated error
+    double riemann_tol;    // plain iterative Riemann solver: stop at this relative change of p
 };
 
 struct DevState {

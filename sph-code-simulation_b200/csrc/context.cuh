@@ -56,6 +56,15 @@ struct sphgpu_ctx {
     bool flist_ready = false;        // built for the current tree and h
     int64_t flist_uses = 0;
 
+    // mixed form's FP64 re-evaluation (recheck.cu): per particle the sum of
+    // |FP32 acceleration terms|, the flags, their scan, the list and its length
+    void* d_recheck = nullptr;
+    float* d_accabs = nullptr;
+    int *d_rflag = nullptr, *d_rpos = nullptr, *d_ridx = nullptr, *d_rcount = nullptr;
+    int recheck_n = 0;
+    bool accabs_valid = false;       // FluidForce filled accabs for the current tree
+    int64_t mixed_rechecks = 0;      // particles re-evaluated in FP64
+
     // host transfer staging (upload / download): one slot of n doubles per
     // field moved, kept across calls
     double* d_stage = nullptr;
@@ -194,6 +203,12 @@ int sr_timestep(sphgpu_ctx* c);
 int sr_predict(sphgpu_ctx* c);
 int sr_correct(sphgpu_ctx* c);
 int gravity_walk_mixed(sphgpu_ctx* c);
+// Mixed form: FluidForce / GravityForce in FP64 for the listed particles
+// (device list of nsub indices), and the pass that lists them (recheck.cu).
+int fluid_force_subset64(sphgpu_ctx* c, const int* idx, int nsub);
+int gravity_subset64(sphgpu_ctx* c, const int* idx, int nsub);
+int ensure_recheck(sphgpu_ctx* c);
+int mixed_recheck(sphgpu_ctx* c);
 int timestep(sphgpu_ctx* c);
 int predict(sphgpu_ctx* c);
 int correct(sphgpu_ctx* c);

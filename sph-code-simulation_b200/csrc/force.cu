@@ -124,7 +124,7 @@ __device__ __forceinline__ void pair_screen(const double* L, const double* R, do
 template <typename T>
 __device__ void riemann_iterative(const double* L, const double* R, double gamma, bool learned, float y, int budget,
                                   double& pstar, double& vstar, int& iters, int& fallback, double scr_ch = -1.0,
-                                  double scr_q1 = 0.0)
+                                  double scr_q1 = 0.0, double tol = 1e-6)
 {
     const double ul = L[0], rhol = L[1], pl = L[2];
     const double ur = R[0], rhor = R[1], pr = R[2];
@@ -178,7 +178,7 @@ __device__ void riemann_iterative(const double* L, const double* R, double gamma
             const double pold = p;
             p = vl_newton_step<double>(p, ul, pl, vl, cl, ur, pr, vr, cr, g1, g2);
             ++iters;
-            if(fabs(p - pold) / p < 1e-6) break;
+            if(fabs(p - pold) / p < tol) break;
         }
     } else {
         float pf = (float)pg;
@@ -191,8 +191,14 @@ __device__ void riemann_iterative(const double* L, const double* R, double gamma
             ++iters;
             if(fabsf(pf - pold) / pf < 1e-6f) break;
         }
-        // final Newton step in FP64
+        // final Newton step in FP64 (more of them down to a tolerance below FP32's)
         p = vl_newton_step<double>((double)pf, ul, pl, vl, cl, ur, pr, vr, cr, g1, g2);
+        for(int it = 0; tol < 1e-6 && it < 20; ++it) {
+            const double pold = p;
+            p = vl_newton_step<double>(p, ul, pl, vl, cl, ur, pr, vr, cr, g1, g2);
+            ++iters;
+            if(fabs(p - pold) / p < tol) break;
+        }
     }
     pstar = p;
     vstar = vl_ustar(p, ul, pl, cl, ur, pr, cr, g1);
@@ -209,12 +215,23 @@ constexpr int force_min_blocks()
     return (sizeof(T) == sizeof(float) || TYPE == SPHGPU_GSPH || TYPE == SPHGPU_GDISPH) ? 4 : 3;
 }
 
+// The particles a launch computes: all n, or (sub.idx != null) the listed
+// ones (the mixed form's FP64 re-evaluation).  count = 0: the launch adds to
+// no work or Riemann counter (the pairs were counted by the first pass).
+struct Subset {
+    const int* idx;
+    int n;
+    int count;
+};
+
 template <typename T, int G, int TYPE, int MODE>
 __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(DevParams P, DevState S, int n, const int* __restrict__ list,
                                                 const int* __restrict__ count, int cap, const double* __restrict__ dtp,
-                                                DevStatus* __restrict__ st, MlpPairs mp, Harvest hv)
+                                                DevStatus* __restrict__ st, MlpPairs mp, Harvest hv,
+                                                float* __restrict__ accabs, Subset sub)
 {
     constexpr int GPW = 32 / G;
+    constexpr bool f32 = sizeof(T) == sizeof(float);
     const int lane = threadIdx.x & (G - 1);
     const long long warp = ((long long)blockIdx.x * FBLK + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * FBLK) >> 5;
@@ -222,10 +239,12 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
     const double gamma = P.gamma;
     unsigned long long solves = 0, iters = 0, fallbacks = 0;
     unsigned n_cand = 0, n_pairs = 0;  // work counters of this lane
+    const int nloop = sub.idx ? sub.n : n;
 
-    for(long long wb = warp * GPW; wb < n; wb += nwarps * GPW) {
-        const int i = (int)(wb + ((threadIdx.x & 31) / G));
-        const bool valid = i < n;
+    for(long long wb = warp * GPW; wb < nloop; wb += nwarps * GPW) {
+        const int slot = (int)(wb + ((threadIdx.x & 31) / G));
+        const bool valid = slot < nloop;
+        const int i = sub.idx ? (valid ? sub.idx[slot] : n) : slot;
         const int cnt = valid ? (MODE == 4 ? mp.dcount[i] : min(count[i], cap)) : 0;
         if(MODE == 4 && !__any_sync(FULL_MASK, cnt > 0)) continue;
         const int* li = list + (size_t)(valid ? i : 0) * (size_t)cap;
@@ -251,6 +270,7 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
         const T mu_inv = T(1) / (mi * ui);
         const T r2i = T(1) / (rhoi * rhoi);
         double ax = 0, ay = 0, az = 0, de = 0;
+        float sabs = 0.f;  // mixed form: sum of |FP32 force terms|, the rounding-error scale
         n_cand += lane < cnt ? (unsigned)((cnt - lane + G - 1) / G) : 0u;
         for(int k = lane; k < cnt; k += G) {
             float yq = 0.f;
@@ -371,7 +391,7 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
                         // the linearised one)
                         const bool learned = (MODE == 3 || MODE == 4) && states_ok;
                         riemann_iterative<T>(Lst, Rst, gamma, learned, MODE == 4 ? yq : __int_as_float(0x7fc00000),
-                                             P.mlp_max_newton, pstar, vstar, it, fb, scr_ch, scr_q1);
+                                             P.mlp_max_newton, pstar, vstar, it, fb, scr_ch, scr_q1, P.riemann_tol);
                         ++solves;
                         iters += it;
                         fallbacks += fb;
@@ -415,6 +435,7 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
                     ax -= fx;
                     ay -= fy;
                     az -= fz;
+                    if constexpr(f32) sabs += (float)(fabs(fx) + fabs(fy) + fabs(fz));
                     de -= fx * (ex * vstar - vi.x) + fy * (ey * vstar - vi.y) + fz * (ez * vstar - vi.z);
                     continue;
                 }
@@ -453,24 +474,30 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
                 a_j = mj * (Pj / (rhoj * rhoj) * (T)sj.z + T(0.5) * pij);
                 e_ = mj * ppr * (T)si.z * vdwi + T(0.5) * mj * pij * vdwij + dac;
             }
-            ax -= (double)(dwi.x * a_i + dwj.x * a_j);
-            ay -= (double)(dwi.y * a_i + dwj.y * a_j);
-            az -= (double)(dwi.z * a_i + dwj.z * a_j);
+            const T fx = dwi.x * a_i + dwj.x * a_j, fy = dwi.y * a_i + dwj.y * a_j, fz = dwi.z * a_i + dwj.z * a_j;
+            ax -= (double)fx;
+            ay -= (double)fy;
+            az -= (double)fz;
             de += (double)e_;
+            if constexpr(f32) sabs += fabsf(fx) + fabsf(fy) + fabsf(fz);
         }
         ax = group_sum<G>(ax);
         ay = group_sum<G>(ay);
         az = group_sum<G>(az);
         de = group_sum<G>(de);
+        if constexpr(f32) sabs = group_sum<G>(sabs);
         if(MODE == 4) {
             if(cnt > 0 && lane == 0) {
                 const double4 a0 = S.acc[i];
                 S.acc[i] = make_double4(a0.x + ax, a0.y + ay, a0.z + az, a0.w + de);
+                if(f32 && accabs) accabs[i] += sabs;
             }
         } else if(valid && lane == 0) {
             S.acc[i] = make_double4(ax, ay, az, de);
+            if(f32 && accabs) accabs[i] = sabs;
         }
     }
+    if(!sub.count) return;
     if(MODE != 4) {  // the completion pass re-solves pairs the force pass counted
         block_count(&st->force_cand, n_cand);
         block_count(&st->force_pairs, n_pairs);
@@ -499,24 +526,27 @@ unsigned force_grid(int n)
 }
 
 template <typename T, int MODE>
-void launch_force(sphgpu_ctx* c, MlpPairs mp, Harvest hv)
+void launch_force(sphgpu_ctx* c, MlpPairs mp, Harvest hv, Subset sub = {nullptr, 0, 1})
 {
-    const unsigned grid = force_grid(c->n);
+    const unsigned grid = force_grid(sub.idx ? sub.n : c->n);
     const int type = c->prm.sph_type;
+    float* accabs = sizeof(T) == sizeof(float) ? c->d_accabs : nullptr;
     if(type == SPHGPU_DISPH) {
         k_force<T, GROUP, SPHGPU_DISPH, 0><<<grid, FBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_plist, c->d_pcount,
-                                                                         (int)c->pcap, c->d_dt, c->d_status, mp, hv);
+                                                                         (int)c->pcap, c->d_dt, c->d_status, mp, hv,
+                                                                         accabs, sub);
     } else if(type == SPHGPU_GSPH) {
         k_force<T, GROUP, SPHGPU_GSPH, MODE><<<grid, FBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_plist,
                                                                            c->d_pcount, (int)c->pcap, c->d_dt,
-                                                                           c->d_status, mp, hv);
+                                                                           c->d_status, mp, hv, accabs, sub);
     } else if(type == SPHGPU_GDISPH) {
         k_force<T, GROUP, SPHGPU_GDISPH, 0><<<grid, FBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_plist,
                                                                           c->d_pcount, (int)c->pcap, c->d_dt,
-                                                                          c->d_status, mp, hv);
+                                                                          c->d_status, mp, hv, accabs, sub);
     } else {
         k_force<T, GROUP, SPHGPU_SSPH, 0><<<grid, FBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_plist, c->d_pcount,
-                                                                        (int)c->pcap, c->d_dt, c->d_status, mp, hv);
+                                                                        (int)c->pcap, c->d_dt, c->d_status, mp, hv,
+                                                                        accabs, sub);
     }
 }
 
@@ -617,6 +647,15 @@ __global__ void k_defer_ranges(const uint64_t* __restrict__ skeys, int n, uint64
 
 }  // namespace
 
+int fluid_force_subset64(sphgpu_ctx* c, const int* idx, int nsub)
+{
+    Harvest hv{};
+    MlpPairs mp{};
+    launch_force<double, 0>(c, mp, hv, Subset{idx, nsub, 0});
+    SPHGPU_LAUNCH_CHECK(c, "FluidForce (FP64 re-evaluation)");
+    return SPHGPU_OK;
+}
+
 int fluid_force(sphgpu_ctx* c)
 {
     if(!c->have_tree) return fail(c, SPHGPU_ERR_STATE, "FluidForce before tree make");
@@ -626,6 +665,10 @@ int fluid_force(sphgpu_ctx* c)
     if(learned && !c->have_mlp) return fail(c, SPHGPU_ERR_NO_MLP, "learned Riemann guess requested without MLP weights");
     const int rc_walk = symmetric_lists(c);
     if(rc_walk < 0) return rc_walk;
+    {
+        const int rc = ensure_recheck(c);
+        if(rc < 0) return rc;
+    }
     stage_begin(c, SPHGPU_T_FORCE);
     Harvest hv{c->d_harvest, c->d_harvest_count, c->harvest_cap, c->harvest_mod, 0u};
     MlpPairs mp{};
@@ -687,6 +730,7 @@ int fluid_force(sphgpu_ctx* c)
     }
     SPHGPU_LAUNCH_CHECK(c, "FluidForce");
     stage_end(c, SPHGPU_T_FORCE, launches);
+    c->accabs_valid = c->prm.precision == SPHGPU_MIXED;
     return rc_walk;
 }
 

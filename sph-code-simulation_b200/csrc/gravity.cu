@@ -29,11 +29,15 @@ namespace {
 
 constexpr int GBLK = 128;
 
+// subset != null: only the listed particles (the mixed form's FP64
+// re-evaluation); those launches add to no work counter.
 __global__ void __launch_bounds__(GBLK) k_gravity(DevParams P, DevState S, DevTree Tr, int n,
-                                                  DevStatus* __restrict__ st)
+                                                  DevStatus* __restrict__ st, const int* __restrict__ subset,
+                                                  int nsub)
 {
-    const int i = blockIdx.x * GBLK + threadIdx.x;
-    const bool valid = i < n;
+    const int slot = blockIdx.x * GBLK + threadIdx.x;
+    const bool valid = slot < (subset ? nsub : n);
+    const int i = subset ? (valid ? subset[slot] : n) : slot;
     double xi = 0, yi = 0, zi = 0, hi = 1;
     double4 acc = make_double4(0, 0, 0, 0);
     if(valid) {
@@ -97,6 +101,7 @@ __global__ void __launch_bounds__(GBLK) k_gravity(DevParams P, DevState S, DevTr
         S.acc[i] = make_double4(ax, ay, az, acc.w);
         S.visc[i].w = phi;
     }
+    if(subset) return;
     block_count(&st->grav_nodes, (unsigned)min(steps, nnodes));
     block_count(&st->grav_mono, n_mono);
     block_count(&st->grav_leaf_pairs, n_leaf);
@@ -136,7 +141,9 @@ __global__ void k_gravity_direct(DevParams P, DevState S, int n, const int* __re
 
 int gravity(sphgpu_ctx* c, bool direct)
 {
-    if(!c->prm.use_gravity) return SPHGPU_OK;
+    // the mixed form's FP64 re-evaluation follows the last module that
+    // writes acc (recheck.cu); GravityForce runs every step, with gravity off too
+    if(!c->prm.use_gravity) return direct ? SPHGPU_OK : mixed_recheck(c);
     if(!direct && !c->have_tree) return fail(c, SPHGPU_ERR_STATE, "GravityForce before tree make");
     if(!direct && c->prm.precision == SPHGPU_MIXED) {
         // the walk's FP32 node records: tree data, timed with the tree
@@ -152,10 +159,18 @@ int gravity(sphgpu_ctx* c, bool direct)
         const int rc = gravity_walk_mixed(c);
         if(rc < 0) return rc;
     } else {
-        k_gravity<<<grid_for(c->n, GBLK), GBLK, 0, c->stream>>>(c->dp, c->s, c->t, c->n, c->d_status);
+        k_gravity<<<grid_for(c->n, GBLK), GBLK, 0, c->stream>>>(c->dp, c->s, c->t, c->n, c->d_status, nullptr, 0);
     }
     SPHGPU_LAUNCH_CHECK(c, "GravityForce");
     stage_end(c, SPHGPU_T_GRAVITY, 1);
+    return direct ? SPHGPU_OK : mixed_recheck(c);
+}
+
+int gravity_subset64(sphgpu_ctx* c, const int* idx, int nsub)
+{
+    if(!c->prm.use_gravity || nsub <= 0) return SPHGPU_OK;
+    k_gravity<<<grid_for(nsub, GBLK), GBLK, 0, c->stream>>>(c->dp, c->s, c->t, c->n, c->d_status, idx, nsub);
+    SPHGPU_LAUNCH_CHECK(c, "GravityForce (FP64 re-evaluation)");
     return SPHGPU_OK;
 }
 

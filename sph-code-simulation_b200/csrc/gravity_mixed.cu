@@ -108,7 +108,7 @@ __device__ __forceinline__ float min_image_f(float d, float L)
 
 __global__ void __launch_bounds__(MBLK, 8) k_gravity_mixed(DevParams P, DevState S, DevTree Tr,
                                                         const GNode* __restrict__ rec, int n,
-                                                        DevStatus* __restrict__ st)
+                                                        DevStatus* __restrict__ st, float* __restrict__ accabs)
 {
     const int i = blockIdx.x * MBLK + threadIdx.x;
     const bool valid = i < n;
@@ -131,6 +131,7 @@ __global__ void __launch_bounds__(MBLK, 8) k_gravity_mixed(DevParams P, DevState
     const float Lx = (float)P.range[0], Ly = (float)P.range[1], Lz = (float)P.range[2];
     double ax = acc.x, ay = acc.y, az = acc.z, phi = 0.0;
     float fx = 0.f, fy = 0.f, fz = 0.f, fp = 0.f;
+    float gabs = 0.f;  // sum of |FP32 terms|, the rounding-error scale of the acceleration
     int since = 0;
     const int nnodes = *Tr.nnodes;
     int nd = valid ? 0 : nnodes, steps = 0;
@@ -163,6 +164,7 @@ __global__ void __launch_bounds__(MBLK, 8) k_gravity_mixed(DevParams P, DevState
             fx -= dx * s;
             fy -= dy * s;
             fz -= dz * s;
+            gabs += s * (fabsf(dx) + fabsf(dy) + fabsf(dz));
         } else if(leaf) {
             const int4 lk = __ldg(&Tr.link[nd]);
             n_leaf += (unsigned)(lk.y - lk.x) - ((i >= lk.x && i < lk.y) ? 1u : 0u);
@@ -184,6 +186,7 @@ __global__ void __launch_bounds__(MBLK, 8) k_gravity_mixed(DevParams P, DevState
                 fx -= rx * c;
                 fy -= ry * c;
                 fz -= rz * c;
+                gabs += fabsf(c) * (fabsf(rx) + fabsf(ry) + fabsf(rz));
             }
         }
         if(++since == FOLD) {
@@ -199,6 +202,7 @@ __global__ void __launch_bounds__(MBLK, 8) k_gravity_mixed(DevParams P, DevState
     if(valid) {
         S.acc[i] = make_double4(ax + (double)fx, ay + (double)fy, az + (double)fz, acc.w);
         S.visc[i].w = phi + (double)fp;
+        if(accabs) accabs[i] += gabs;
     }
     block_count(&st->grav_nodes, (unsigned)min(steps, nnodes));
     block_count(&st->grav_mono, n_mono);
@@ -224,7 +228,7 @@ int gravity_walk_mixed(sphgpu_ctx* c)
 {
     if(c->gnode_cap < c->node_cap) return fail(c, SPHGPU_ERR_STATE, "mixed gravity walk before its node records");
     k_gravity_mixed<<<grid_for(c->n, MBLK), MBLK, 0, c->stream>>>(
-        c->dp, c->s, c->t, static_cast<const GNode*>(c->d_gnode), c->n, c->d_status);
+        c->dp, c->s, c->t, static_cast<const GNode*>(c->d_gnode), c->n, c->d_status, c->d_accabs);
     return SPHGPU_OK;
 }
 

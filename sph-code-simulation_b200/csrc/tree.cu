@@ -483,6 +483,7 @@ __global__ void k_ksize_up(int n, const int* __restrict__ leaf_of_start, DevTree
 int tree_make(sphgpu_ctx* c)
 {
     c->flist_ready = false;
+    c->accabs_valid = false;
     const int n = c->n;
     cudaStream_t st = c->stream;
     if(n <= 0) return fail(c, SPHGPU_ERR_STATE, "tree_make: no particles");

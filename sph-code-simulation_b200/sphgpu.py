@@ -29,7 +29,7 @@ from sphparams import (CUBIC_SPLINE, DISPH, FIELD_INDEX, FIELDS, FP64, GAUSSIAN,
                        GUESS_MLP, GUESS_NONE, MIXED, NFIELDS, RIEMANN_HLL, RIEMANN_ITERATIVE, SRGSPH, SSPH,
                        WENDLAND, Params, config_params)
 STAGES = ["timestep", "predict", "tree", "gather_walk", "pre", "set_kernel", "pair_walk",
-          "force", "gravity", "correct"]
+          "force", "gravity", "correct", "recheck"]
 
 
 class SPHException(RuntimeError):
@@ -91,7 +91,7 @@ class Counters(C.Structure):
         "gather_capacity", "max_gather", "max_pair", "node_count", "retries", "walk_group_warps",
         "walk_split_warps", "walk_fallbacks", "mlp_guesses", "force_list_builds", "pre_candidates",
         "pre_newton_pairs", "pre_pairs", "force_candidates", "force_pairs", "gravity_nodes",
-        "gravity_monopoles", "gravity_leaf_pairs")]
+        "gravity_monopoles", "gravity_leaf_pairs", "mixed_rechecks")]
 
 
 _lib = None

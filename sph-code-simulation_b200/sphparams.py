@@ -49,7 +49,7 @@ class Params(C.Structure):
         ("riemann_solver", C.c_int32), ("precision", C.c_int32), ("riemann_guess", C.c_int32),
         ("mlp_max_newton", C.c_int32), ("sr_2nd_order", C.c_int32), ("tree_root_origin", C.c_int32),
         ("sr_c_speed", C.c_double), ("sr_c_shock", C.c_double), ("sr_c_cd", C.c_double), ("sr_eta", C.c_double),
-        ("sr_c_smooth", C.c_double),
+        ("sr_c_smooth", C.c_double), ("mixed_acc_tol", C.c_double), ("riemann_tol", C.c_double),
     ]
 
     def copy(self) -> "Params":
@@ -72,7 +72,7 @@ DEFAULTS = dict(
     leaf_particle_num=1, periodic=0, use_gravity=0, gsph_2nd_order=1, g_constant=1.0, theta=0.5,
     riemann_solver=RIEMANN_HLL, precision=FP64, riemann_guess=GUESS_NONE, mlp_max_newton=4,
     sr_2nd_order=1, tree_root_origin=1, sr_c_speed=1.0, sr_c_shock=3.0, sr_c_cd=1.0, sr_eta=1.0,
-    sr_c_smooth=2.0,
+    sr_c_smooth=2.0, mixed_acc_tol=0.0, riemann_tol=1e-6,
 )
 
 
@@ -117,6 +117,10 @@ def config_params(name: str, **overrides) -> Params:
         p = defaults(sph_type=SRGSPH, kernel=CUBIC_SPLINE, neighbor_number=50, sr_2nd_order=1,
                      gamma=5.0 / 3.0, periodic=1, range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.05, 0.05),
                      sr_c_speed=1.0, sr_c_shock=3.0, sr_c_cd=1.0, sr_eta=1.0, sr_c_smooth=2.0)
+    elif name == "blast_gsph":         # gsph many-blast cube, MUSCL, iterative Riemann, cubic, K=50
+        p = defaults(sph_type=GSPH, kernel=CUBIC_SPLINE, neighbor_number=50, gsph_2nd_order=1,
+                     riemann_solver=RIEMANN_ITERATIVE, gamma=1.4, periodic=1,
+                     range_min=(-0.5, -0.5, -0.5), range_max=(0.5, 0.5, 0.5))
     elif name == "evrard_disph":       # disph + gravity sphere, Wendland, K=128, TD-AV, AC
         p = defaults(sph_type=DISPH, kernel=WENDLAND, neighbor_number=128, use_time_dependent_av=1,
                      alpha_min=0.1, alpha_max=2.0, epsilon_av=0.2, use_balsara_switch=1, use_ac=1,
