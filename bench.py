@@ -76,6 +76,10 @@ def _tube(n):
     return ics.shock_tube((0.05 * 0.05 / n) ** (1.0 / 3.0), ly=0.05)
 
 
+def _blast(n):
+    return ics.blast_field(1.0 / round(n ** (1.0 / 3.0)))
+
+
 WORKLOADS = {
     "evrard_ssph": Workload("evrard_ssph", "ssph Evrard sphere 17K (cubic, K=50, leaf=1, Balsara, BH gravity)",
                             "evrard_ssph", _evrard, 17256, 17256),
@@ -87,6 +91,15 @@ WORKLOADS = {
                               "tube_gsph", _tube, 2.0e6, 6.5e4, learned=True),
     "tube_gdisph": Workload("tube_gdisph", "gdisph shock tube 2.0M (MUSCL + HLL, cubic, K=50, Balsara, TD-AV, AC)",
                             "tube_gdisph", _tube, 2.0e6, 6.5e4),
+    # many point blasts: most pairs are strong-shock Riemann problems (plain
+    # solver ~3.5 Newton iterations per solve); the learned start against
+    # the plain solver at the reference's 1e-6 and at the learned path's 1e-10
+    "blast_gsph": Workload("blast_gsph", "gsph many-blast cube 2.0M (MUSCL, iterative Riemann, cubic, K=50)",
+                           "blast_gsph", _blast, 2.0e6, 1.3e5),
+    "blast_gsph_tol1e-10": Workload("blast_gsph_tol1e-10", "gsph many-blast cube 2.0M, plain solver to 1e-10",
+                                    "blast_gsph", _blast, 2.0e6, 1.3e5, riemann_tol=1e-10),
+    "blast_gsph_mlp": Workload("blast_gsph_mlp", "gsph many-blast cube 2.0M with the learned Riemann guess",
+                               "blast_gsph", _blast, 2.0e6, 1.3e5, learned=True),
     # The disph sphere's centre breaks down at t ~ 0.003 on this resolution
     # (innermost particles reach u < 0 in predict: the scheme, reproduced by
     # the compiled reference); cflSound 0.006 / cflForce 0.003 keep every

@@ -190,6 +190,44 @@ __device__ __forceinline__ double abs2x(Vec3d d)
     return xadd(xadd(xmul(d.x, d.x), xmul(d.y, d.y)), xmul(d.z, d.z));
 }
 
+// The reference's pair predicate r < h with r = sqrt(r^2) correctly rounded
+// (src/pre_interaction.cpp:89, src/fluid_force.cpp:62), decided from r^2:
+// outside a band of relative width 2^-40 around h^2 the rounding of the root
+// cannot change the answer (2^-40 is far above the 2^-53 rounding of h * h and
+// of the root), so the square root is taken only inside the band.
+__device__ __forceinline__ bool root_lt(double r2, double h)
+{
+    const double h2 = h * h;
+    if(r2 < h2 * (1.0 - 0x1p-40)) return true;
+    if(r2 > h2 * (1.0 + 0x1p-40)) return false;
+    return sqrt(r2) < h;
+}
+
+// Pair loops: true when sqrt(r2) < h (exactly as root_lt); then r and 1/r.
+// Outside the band they come from one reciprocal square root (CUDA's rsqrt,
+// within an ulp of 1/sqrt), inside it from the correctly rounded root; for
+// r2 = 0 both are 0.  The pair sums built from them agree with the
+// reference's to rounding, as before; only set membership must be exact.
+__device__ __forceinline__ bool pair_within(double r2, double h, double& r, double& rinv)
+{
+    const double h2 = h * h;
+    if(r2 > h2 * (1.0 + 0x1p-40)) return false;
+    if(r2 >= h2 * (1.0 - 0x1p-40)) {
+        r = sqrt(r2);
+        if(!(r < h)) return false;
+        rinv = r > 0.0 ? 1.0 / r : 0.0;
+        return true;
+    }
+    if(r2 > 0.0) {
+        rinv = rsqrt(r2);
+        r = r2 * rinv;
+    } else {
+        r = 0.0;
+        rinv = 0.0;
+    }
+    return true;
+}
+
 // ------------------------------------------------------------ SPH kernels
 // W, grad W (as the scalar c with grad W = r_ij c) and dW/dh for the cubic
 // spline (include/kernel/cubic_spline.hpp:21-53), Wendland C4

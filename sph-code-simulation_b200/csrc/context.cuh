@@ -87,6 +87,7 @@ struct sphgpu_ctx {
     void* d_mlp_defer = nullptr;
     int64_t mlp_rcap = 0;             // rows the allocation holds
     int64_t mlp_ncap = 0;             // particles the allocation holds
+    int64_t mlp_rows_demand = 0;      // rows the last learned force pass asked for
     // mixed-precision gravity: 32-byte FP32 node records of the current tree
     void* d_gnode = nullptr;
     int gnode_cap = 0;

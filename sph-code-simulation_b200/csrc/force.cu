@@ -289,8 +289,9 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
             if(r >= (hi < hj ? hj : hi) || r == 0.0) continue;
             ++n_pairs;
             const double4 tj = S.thermo[j];
+            const double rinv = 1.0 / r;
             const T rT = (T)r;
-            const T rinvT = (T)(1.0 / r);
+            const T rinvT = (T)rinv;
             const V3<T> rv{(T)d.x, (T)d.y, (T)d.z};
             const KernH<T> khj(P.kernel, (T)hj);
             const T ci_ = khi.dwc(rT, rinvT);
@@ -304,7 +305,6 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
             // (src/gdisph/gd_fluid_force.cpp:95-178)
             T psi = T(1), psj = T(1);
             if(TYPE == SPHGPU_GSPH || TYPE == SPHGPU_GDISPH) {
-                const double rinv = 1.0 / r;
                 const double ex = d.x * rinv, ey = d.y * rinv, ez = d.z * rinv;
                 const double vei = vi.x * ex + vi.y * ey + vi.z * ez;
                 const double vej = vj.x * ex + vj.y * ey + vj.z * ez;
@@ -677,7 +677,11 @@ int fluid_force(sphgpu_ctx* c)
         const int64_t slots = (int64_t)c->n * c->pcap;
         if(slots > 0xFFFFFFFFLL) return fail(c, SPHGPU_ERR_ARG, "learned guess: more than 2^32 pair slots");
         // room for 1/16 of all pair slots (the screen rejects well under 1%)
-        const int64_t rcap = std::max<int64_t>(1 << 20, slots / 16);
+        // room for 1/16 of all pair slots, or for 1.25x the rows the last call
+        // asked for (many strong shocks), at most one row per slot
+        const int64_t rcap = std::min<int64_t>(
+            std::max<int64_t>(std::max<int64_t>(1 << 20, slots / 16), c->mlp_rows_demand + c->mlp_rows_demand / 4),
+            std::max<int64_t>(slots, 1 << 20));
         if(rcap > c->mlp_rcap || c->n > c->mlp_ncap) {
             if(c->d_mlp_defer) cudaFree(c->d_mlp_defer);
             c->d_mlp_defer = nullptr;
@@ -700,6 +704,7 @@ int fluid_force(sphgpu_ctx* c)
         unsigned long long rows = 0;
         SPHGPU_CUDA(c, cudaMemcpyAsync(&rows, L.rows, sizeof(rows), cudaMemcpyDeviceToHost, c->stream));
         SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+        c->mlp_rows_demand = (int64_t)rows;  // the next call sizes its rows by it
         rows = std::min<unsigned long long>(rows, (unsigned long long)c->mlp_rcap);
         if(rows > 0) {
             const int nr = (int)rows;

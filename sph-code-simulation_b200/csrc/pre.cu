@@ -45,16 +45,20 @@ __device__ __forceinline__ double exact_r(const DevParams& P, double xi, double 
     return sqrt(abs2x(d));
 }
 
-// r = |r_ij| with the reference's rounding (sqrt of the unfused r^2), or -1
-// when r^2 exceeds h^2 (1 + 2^-40): then the correctly rounded sqrt is above
-// h, so r < h is false and the square root is skipped.
-__device__ __forceinline__ double r_within(const DevParams& P, double xi, double yi, double zi, double4 pj, double h,
-                                           Vec3d& d)
+// The Newton sweep's pair test and distance: true when r < h exactly as the
+// reference decides it (root_lt on the unfused FP64 r^2); r in the sweep's
+// precision (FP64: rsqrt-based, FP32: from the FP32 r^2).
+__device__ __forceinline__ bool sweep_r(double r2, double h, double& r)
 {
-    d = rij(P, xi, yi, zi, pj.x, pj.y, pj.z);
-    const double r2 = abs2x(d);
-    if(r2 > h * h * (1.0 + 0x1p-40)) return -1.0;
-    return sqrt(r2);
+    double rinv;
+    return pair_within(r2, h, r, rinv);
+}
+__device__ __forceinline__ bool sweep_r(double r2, double h, float& r)
+{
+    if(!root_lt(r2, h)) return false;
+    const float r2f = (float)r2;
+    r = r2f > 0.f ? r2f * rsqrtf(r2f) : 0.f;
+    return true;
 }
 
 // Minimum resident blocks per SM (caps registers; measured on B200).
@@ -112,12 +116,11 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
                     const int jc = jn;
                     if(k + G < cnt) jn = __ldg(&li[k + G]);
                     const double4 pj = S.pos[jc];
-                    Vec3d dv;
-                    const double r = r_within(P, pi.x, pi.y, pi.z, pj, h, dv);
-                    if(r >= 0.0 && r < h) {
+                    T rT;
+                    if(sweep_r(abs2x(rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z)), h, rT)) {
                         ++n_newton;
-                        const T w = kh.w((T)r);
-                        const T dh = kh.dhw((T)r);
+                        const T w = kh.w(rT);
+                        const T dh = kh.dhw(rT);
                         if(disph) {
                             d += w;
                             dd += dh;
@@ -158,14 +161,13 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
             const int j = jn2;
             if(k + G < cnt) jn2 = __ldg(&li[k + G]);
             const double4 pj = S.pos[j];
-            Vec3d dv;
-            const double r = r_within(P, pi.x, pi.y, pi.z, pj, h, dv);
-            if(!(r >= 0.0 && r < h)) continue;
+            const Vec3d dv = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
+            double r, rinv;
+            if(!pair_within(abs2x(dv), h, r, rinv)) continue;
             ++nn;
             const double4 vj = S.vel[j];
             const double4 tj = S.thermo[j];
             const T rT = (T)r;
-            const double rinv = r > 0.0 ? 1.0 / r : 0.0;
             const T w = kh.w(rT);
             const T mj = (T)pj.w;
             if(disph) {
