@@ -436,7 +436,7 @@ def _hbm_roofline(G, sim, stages, counters, n, args, hbm, peak_kind):
         algo = nodes * nb + n * 32 + entries * 4 + n * 4
         note = "node table + positions read once, list entries written once"
     elif dom == "pre":
-        algo = counters["pre_candidates"] / max(args.steps, 1) * 4 / 3 + n * (96 + 72)
+        algo = counters["pre_list_entries"] / max(args.steps, 1) * 4 + n * (96 + 72)
         note = "gather list + particle state read once, outputs written once"
     elif dom == "force":
         algo = counters["force_candidates"] / max(args.steps, 1) * 4 + n * (128 + 32)

@@ -128,6 +128,14 @@ typedef struct sphgpu_params {
      * the same Newton iteration further, for like-for-like comparisons with
      * the learned start, which always refines to 1e-10).  (1e-6)          */
     double  riemann_tol;
+    /* No counterpart in the reference (an implementation choice with the
+     * same results): the gather walk builds lists of radius (1 + gather_skin)
+     * times the gather radius and later steps reuse them, moved to each new
+     * tree's particle order, while every particle's gather sphere stays
+     * inside its list's sphere (displacements are tracked); the consumers
+     * take exactly the reference's list members from them.  0 = a fresh
+     * exact walk every step.  (0.02)                                      */
+    double  gather_skin;
 } sphgpu_params;
 
 /* Per-particle fields, in the order of sph::SPHParticle where it has them
@@ -177,6 +185,8 @@ typedef struct sphgpu_counters {
                                       the Newton sweeps and the final pass  */
     int64_t pre_newton_pairs;      /* pairs inside h in the Newton sweeps    */
     int64_t pre_pairs;             /* pairs inside h in the final pass       */
+    int64_t pre_list_entries;      /* gather-list entries read by the final pass
+                                      (each list once)                       */
     int64_t force_candidates;      /* pair-list entries tested by FluidForce */
     int64_t force_pairs;           /* pairs inside max(h_i, h_j)             */
     int64_t gravity_nodes;         /* tree nodes met (opening tests)         */
@@ -185,6 +195,8 @@ typedef struct sphgpu_counters {
     int64_t mixed_rechecks;        /* mixed form: particles whose FluidForce and
                                       GravityForce were re-evaluated in FP64
                                       (mixed_acc_tol)                       */
+    int64_t skin_builds;           /* gather walks that built skin lists      */
+    int64_t skin_reuses;           /* steps that reused them (no walk)        */
 } sphgpu_counters;
 
 /* Stage timers (ms, summed since the last reset; CUDA events on the

@@ -97,6 +97,7 @@ int ensure_list_capacity(sphgpu_ctx* c, int which, int64_t cap)
     int*& list = which == 0 ? c->d_glist : c->d_plist;
     int64_t& cur = which == 0 ? c->gcap : c->pcap;
     if(cap <= cur && list) return SPHGPU_OK;
+    if(which == 0) c->skin_valid = false;  // the skin buffers no longer match
     if(list) {
         SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
         SPHGPU_CUDA(c, cudaFree(list));
@@ -129,6 +130,7 @@ void set_dev_params(sphgpu_ctx* c)
     d.sr_c_smooth = p.sr_c_smooth;
     d.mixed_acc_tol = p.mixed_acc_tol;
     d.riemann_tol = p.riemann_tol;
+    d.gather_skin = p.gather_skin;
     d.av_alpha = p.av_alpha;
     d.balsara = p.use_balsara_switch;
     d.td_av = p.use_time_dependent_av;
@@ -169,6 +171,13 @@ void free_all(sphgpu_ctx* c)
     if(c->d_stage) cudaFree(c->d_stage);
     c->d_stage = nullptr;
     c->stage_cap = 0;
+    if(c->d_glist_alt) cudaFree(c->d_glist_alt);
+    if(c->d_skin) cudaFree(c->d_skin);
+    c->d_glist_alt = nullptr;
+    c->d_skin = nullptr;
+    c->skin_n = 0;
+    c->skin_cap = 0;
+    c->skin_valid = false;
 }
 
 template <typename T>
@@ -206,7 +215,8 @@ int alloc_all(sphgpu_ctx* c, int n)
        || (rc = dalloc(c, c->t.link, nc)) || (rc = dalloc(c, c->t.parent, nc)) || (rc = dalloc(c, c->t.nchild, nc))
        || (rc = dalloc(c, c->t.child, 8 * (size_t)nc))
        || (rc = dalloc(c, c->t.counter, nc)) || (rc = dalloc(c, c->t.nnodes, 4))
-       || (rc = dalloc(c, c->t.leaf_of, n)) || (rc = dalloc(c, c->t.pks, n)))
+       || (rc = dalloc(c, c->t.leaf_of, n)) || (rc = dalloc(c, c->t.pks, n)) || (rc = dalloc(c, c->t.qpos, n))
+       || (rc = dalloc(c, c->t.qbad, 1)))
         return rc;
     if((rc = dalloc(c, c->d_root, 1)) || (rc = dalloc(c, c->d_bbox_part, 6 * 1024)) || (rc = dalloc(c, c->d_keys, n))
        || (rc = dalloc(c, c->d_keys_alt, n)) || (rc = dalloc(c, c->d_vals, n)) || (rc = dalloc(c, c->d_vals_alt, n))
@@ -427,6 +437,7 @@ int check_params(const sphgpu_params* p, std::string& why)
     if(p->precision != SPHGPU_FP64 && p->precision != SPHGPU_MIXED) return why = "precision must be fp64 or mixed", -1;
     if(!(p->mixed_acc_tol >= 0.0)) return why = "mixed_acc_tol must be >= 0", -1;
     if(!(p->riemann_tol > 0.0 && p->riemann_tol < 1.0)) return why = "riemann_tol must be in (0, 1)", -1;
+    if(!(p->gather_skin >= 0.0 && p->gather_skin <= 1.0)) return why = "gather_skin must be in [0, 1]", -1;
     return 0;
 }
 
@@ -475,6 +486,7 @@ void sphgpu_default_params(sphgpu_params* p)
     p->sr_c_smooth = 2.0;
     p->mixed_acc_tol = 0.0;
     p->riemann_tol = 1e-6;
+    p->gather_skin = 0.02;
 }
 
 int sphgpu_device_ok(void)
@@ -567,6 +579,7 @@ int sphgpu_upload(sphgpu_ctx* c, int64_t n, const double* const* fields)
     c->have_tree = false;
     c->flist_ready = false;
     c->first_pre = true;
+    c->skin_valid = false;
     c->time = 0.0;
     return SPHGPU_OK;
 }
@@ -847,6 +860,7 @@ int sphgpu_set_walk_mode(sphgpu_ctx* c, int mode)
 {
     if(!c || mode < 0 || mode > 1) return SPHGPU_ERR_ARG;
     c->walk_mode = mode;
+    c->skin_valid = false;
     return SPHGPU_OK;
 }
 
@@ -854,6 +868,7 @@ int sphgpu_set_initial_smoothing(sphgpu_ctx* c, int on)
 {
     if(!c) return SPHGPU_ERR_ARG;
     c->first_pre = on != 0;
+    if(c->first_pre) c->skin_valid = false;
     return SPHGPU_OK;
 }
 
@@ -915,12 +930,15 @@ int sphgpu_get_counters(sphgpu_ctx* c, sphgpu_counters* o)
     o->pre_candidates = (int64_t)c->h_status.pre_cand;
     o->pre_newton_pairs = (int64_t)c->h_status.pre_newton_pairs;
     o->pre_pairs = (int64_t)c->h_status.pre_pairs;
+    o->pre_list_entries = (int64_t)c->h_status.pre_list;
     o->force_candidates = (int64_t)c->h_status.force_cand;
     o->force_pairs = (int64_t)c->h_status.force_pairs;
     o->gravity_nodes = (int64_t)c->h_status.grav_nodes;
     o->gravity_monopoles = (int64_t)c->h_status.grav_mono;
     o->gravity_leaf_pairs = (int64_t)c->h_status.grav_leaf_pairs;
     o->mixed_rechecks = c->mixed_rechecks;
+    o->skin_builds = c->skin_builds;
+    o->skin_reuses = c->skin_reuses;
     return SPHGPU_OK;
 }
 
@@ -934,6 +952,8 @@ int sphgpu_reset_counters(sphgpu_ctx* c)
     std::memset(&c->h_status, 0, sizeof(c->h_status));
     c->retries = 0;
     c->mixed_rechecks = 0;
+    c->skin_builds = 0;
+    c->skin_reuses = 0;
     return SPHGPU_OK;
 }
 

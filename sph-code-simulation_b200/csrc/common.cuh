@@ -49,6 +49,7 @@ struct DevParams {
     double sr_c, sr_c_shock, sr_c_cd, sr_eta, sr_c_smooth;
     double mixed_acc_tol;  // mixed form: FP64 re-evaluation above this estimated error
     double riemann_tol;    // plain iterative Riemann solver: stop at this relative change of p
+    double gather_skin;    // skin of the reused gather lists (0 = exact walk every step)
 };
 
 struct DevState {
@@ -79,6 +80,8 @@ struct DevTree {
     int* nnodes;     // device scalar: total node count (root included)
     int* leaf_of;    // per particle (tree order): the leaf holding it
     double* pks;     // per particle: kernel_size of its leaf (set_kernel)
+    int4* qpos;      // per particle: quantised position and FP32 mass (QFrame)
+    int* qbad;       // device scalar: nonzero = a particle lies outside the QFrame
 };
 
 // Packed status words read back by the host after a module.
@@ -102,6 +105,7 @@ struct DevStatus {
     unsigned long long pre_cand;           // gather-list candidates tested (every sweep + fused pass)
     unsigned long long pre_newton_pairs;   // pairs inside h in the Newton sweeps
     unsigned long long pre_pairs;          // pairs inside h in the fused pass
+    unsigned long long pre_list;           // gather-list entries (each list read once: the fused pass)
     unsigned long long force_cand;         // pair-list entries tested by FluidForce
     unsigned long long force_pairs;        // pairs inside max(h_i, h_j)
     unsigned long long grav_nodes;         // nodes met by the gravity walk (opening tests)
@@ -190,6 +194,43 @@ __device__ __forceinline__ double abs2x(Vec3d d)
     return xadd(xadd(xmul(d.x, d.x), xmul(d.y, d.y)), xmul(d.z, d.z));
 }
 
+// Membership of j in the reference's gather list of i (radius R), for a
+// particle whose h reaches R - delta while its candidates come from a skin
+// list (a superset): r^2 < R^2 and, within delta of the radius, the
+// reference's box tests up the path from j's leaf (src/bhtree.cpp:277-316), in
+// unfused FP64 as the walk evaluates them.  Rare.
+__device__ __forceinline__ bool gather_member_x(const double4* __restrict__ geo, const int* __restrict__ parent,
+                                             const int* __restrict__ leaf_of, int periodic, double Lx, double Ly,
+                                             double Lz, double xi, double yi, double zi, double R, double delta, int j,
+                                             double r2)
+{
+    if(!(r2 < xmul(R, R))) return false;
+    const double hs = R - delta;
+    if(hs > 0.0 && r2 < xmul(hs, hs)) return true;
+    int A = __ldg(&leaf_of[j]);
+    for(int up = 0; A >= 0 && up < 64; ++up) {
+        const double4 g = ldg4(&geo[A]);
+        const double e = xadd(xmul(g.w, 0.5), R);
+        double dx = xsub(xi, g.x), dy = xsub(yi, g.y), dz = xsub(zi, g.z);
+        if(periodic) {
+            dx = min_image(dx, Lx);
+            dy = min_image(dy, Ly);
+            dz = min_image(dz, Lz);
+        }
+        const double m = fmax(fmax(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
+        if(!(m <= xmul(e, e))) return false;
+        A = A == 0 ? -1 : __ldg(&parent[A]);
+    }
+    return true;
+}
+
+__device__ __forceinline__ bool gather_member(const DevParams& P, const DevTree& T, double xi, double yi, double zi,
+                                              double R, double delta, int j, double r2)
+{
+    return gather_member_x(T.geo, T.parent, T.leaf_of, P.periodic, P.range[0], P.range[1], P.range[2], xi, yi, zi,
+                           R, delta, j, r2);
+}
+
 // The reference's pair predicate r < h with r = sqrt(r^2) correctly rounded
 // (src/pre_interaction.cpp:89, src/fluid_force.cpp:62), decided from r^2:
 // outside a band of relative width 2^-40 around h^2 the rounding of the root
@@ -201,6 +242,85 @@ __device__ __forceinline__ bool root_lt(double r2, double h)
     if(r2 < h2 * (1.0 - 0x1p-40)) return true;
     if(r2 > h2 * (1.0 + 0x1p-40)) return false;
     return sqrt(r2) < h;
+}
+
+// ---------------------------------------------------------------------------
+// Quantised positions: 16-byte records {qx, qy, qz, mass as float bits} that
+// the pair loops classify most candidates from in FP32, loading the 32-byte
+// FP64 position only for the few whose answer the FP32 bound leaves open.
+// Per axis q = round((x - lo) s) as a 32-bit integer; differences are taken in
+// wrapping integer arithmetic, so on a periodic axis (s = 2^32 / L) they are
+// the minimum image, and on an open axis (the root box, a little widened,
+// mapped onto [0, 2^31)) they never overflow.  A quantum is 2^-31 of the box
+// (2^-32 periodic); the mixed form's smoothing-length sweeps take their
+// distances from these records too, every other pair term from FP64
+// positions.  Error of the FP32
+// difference d' = float(q_i - q_j) * float(1 / s) against the exact difference
+// d, per axis: |d' - d| <= 1.01 / s + 3.1 * 2^-24 |d| (two rounding halves of
+// q, the conversion, 1 / s and the product in FP32); the FP32 sum of squares
+// adds 3 * 2^-24.  So with a = 2 / s:
+//   r2f <  ((h - a)(1 - 2^-20))^2  (rounded down to FP32)  =>  |d| < h (1 - 2^-21)
+//   r2f >= ((h + a)(1 + 2^-20))^2  (rounded up)            =>  |d| > h (1 + 2^-21)
+// and the reference's FP64 r (sqrt of the rounded r^2, ~3 * 2^-53 |d| from
+// |d|) then compares with h the same way.  Everything between, and every
+// pair with an axis difference of 2^30 quanta or more (where a periodic
+// axis's image could differ from the reference's choice), takes the FP64
+// test.  DevTree::qbad (a particle outside the frame) sends every pair to the
+// FP64 test.
+struct QFrame {
+    double lo[3], s[3];
+    float inv[3];
+    double a;  // 2 / min(s): the absolute part of the bound
+};
+
+__device__ __forceinline__ QFrame qframe(const DevParams& P, const double4* __restrict__ geo)
+{
+    QFrame f;
+    if(P.periodic) {
+        for(int k = 0; k < 3; ++k) {
+            f.lo[k] = P.lo[k];
+            f.s[k] = 0x1p32 / P.range[k];
+        }
+    } else {
+        // the root box widened by 2^-8 of its edge, mapped onto [0, 2^31)
+        const double4 g = geo[0];
+        const double span = (g.w > 0.0 ? g.w : 1.0) * (1.0 + 0x1p-8);
+        f.lo[0] = g.x - 0.5 * span;
+        f.lo[1] = g.y - 0.5 * span;
+        f.lo[2] = g.z - 0.5 * span;
+        f.s[0] = f.s[1] = f.s[2] = 0x1p31 * (1.0 - 0x1p-8) / span;
+    }
+    for(int k = 0; k < 3; ++k) f.inv[k] = (float)(1.0 / f.s[k]);
+    f.a = 2.0 / fmin(f.s[0], fmin(f.s[1], f.s[2]));
+    return f;
+}
+
+// FP32 thresholds of the classification above for radius h: x = inside
+// below, y = outside at or above.
+__device__ __forceinline__ float2 qthresh(const QFrame& f, double h)
+{
+    const double lo = (h - f.a) * (1.0 - 0x1p-20);
+    const double hi = (h + f.a) * (1.0 + 0x1p-20);
+    return make_float2(lo > 0.0 ? __double2float_rd(lo * lo) : 0.f, __double2float_ru(hi * hi));
+}
+
+// The FP32 difference of two quantised positions; false when an axis
+// difference reaches 2^30 quanta (the FP64 test decides such pairs).
+__device__ __forceinline__ bool qdiff(const QFrame& f, int4 qi, int4 qj, float& dx, float& dy, float& dz)
+{
+    const int ix = (int)((unsigned)qi.x - (unsigned)qj.x);
+    const int iy = (int)((unsigned)qi.y - (unsigned)qj.y);
+    const int iz = (int)((unsigned)qi.z - (unsigned)qj.z);
+    dx = (float)ix * f.inv[0];
+    dy = (float)iy * f.inv[1];
+    dz = (float)iz * f.inv[2];
+    constexpr unsigned B = 1u << 30;
+    return ((unsigned)ix + B < 2u * B) & ((unsigned)iy + B < 2u * B) & ((unsigned)iz + B < 2u * B);
+}
+
+__device__ __forceinline__ float qr2(float dx, float dy, float dz)
+{
+    return fmaf(dx, dx, fmaf(dy, dy, __fmul_rn(dz, dz)));
 }
 
 // Pair loops: true when sqrt(r2) < h (exactly as root_lt); then r and 1/r.
@@ -428,6 +548,17 @@ __device__ __forceinline__ T warp_min(T v)
     for(int o = 16; o > 0; o >>= 1) {
         const T u = __shfl_xor_sync(FULL_MASK, v, o);
         v = u < v ? u : v;
+    }
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_max_pos(T v)
+{
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1) {
+        const T u = __shfl_xor_sync(FULL_MASK, v, o);
+        v = u > v ? u : v;
     }
     return v;
 }

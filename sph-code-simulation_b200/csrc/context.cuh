@@ -48,6 +48,20 @@ struct sphgpu_ctx {
     int* d_plist = nullptr;          // symmetric list (FluidForce)
     int* d_pcount = nullptr;
     int64_t pcap = 0;
+    // skin (Verlet) gather lists (walk.cu): a second list buffer, and per
+    // particle the walk radius and position of the build
+    int* d_glist_alt = nullptr;      // own allocation; trades places with d_glist
+    void* d_skin = nullptr;          // the rest, one allocation
+    int* d_gcount_alt = nullptr;
+    double *d_skin_r = nullptr, *d_skin_r_alt = nullptr;
+    double4 *d_skin_x = nullptr, *d_skin_x_alt = nullptr;
+    int* d_skin_new = nullptr;       // old position -> new position of the last permutation
+    double* d_skin_scal = nullptr;   // largest displacement, failed-check flag
+    int skin_n = 0;
+    int64_t skin_cap = 0;
+    bool skin_valid = false;         // d_glist holds skin lists of the current order
+    double skin_delta_now = 0.0;     // the walk's safety margin for the current tree
+    int64_t skin_builds = 0, skin_reuses = 0;
     // pair lists built from the gather lists (flist.cu)
     int* d_tcount = nullptr;         // entries appended to each row from the back
     int* d_flist_flags = nullptr;    // {incomplete, longest list, over neighborNumber * 1000}
@@ -182,6 +196,12 @@ void stage_flush(sphgpu_ctx* c);   // call only after the stream is idle
 int tree_make(sphgpu_ctx* c);
 int tree_set_kernel(sphgpu_ctx* c);
 int gather_walk(sphgpu_ctx* c, bool compute_guess, double ratio);
+// The step's gather lists: skin lists reused when still valid, else built
+// (gather_skin > 0), or the exact walk (walk.cu).
+int gather_lists(sphgpu_ctx* c, double ratio);
+// Move valid skin lists to the order of a new tree (src: old position of the
+// particle now at each position).
+int skin_permute(sphgpu_ctx* c, const uint32_t* src);
 int pair_walk(sphgpu_ctx* c);
 int export_lists(sphgpu_ctx* c, int which, int64_t* offsets, int32_t* ids, int64_t cap);
 int exhaustive_lists(sphgpu_ctx* c, int is_ij, int64_t* offsets, int32_t* ids, int64_t cap);

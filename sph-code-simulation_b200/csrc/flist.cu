@@ -10,6 +10,10 @@
 //   transposed(i) = { j : i in gather(j), r_ij < h_j, not r_ij < h_i }
 // because r < h <= R implies r^2 < R^2 for correctly rounded r = sqrt(r^2),
 // and r_ij = r_ji bit for bit (exact negation, antisymmetric minimum image).
+// From a skin list (built at a wider radius, reused over steps: a superset of
+// the gather list) own(i) keeps the gather list's members only: every r < h_i
+// when h_i < R_i - delta (delta = the walk's margin), else those that pass the
+// exact membership test (gather_member).
 // Each particle scans its gather list once: own entries go to the front of its
 // row in gather-list order (group ballot compaction), and each pair that only
 // the neighbour's kernel reaches is appended to the neighbour's row from the
@@ -17,6 +21,9 @@
 // index (a deterministic summation order) and moves them behind the own
 // entries.  If some h_k > R_k, or a row does not fit, the step falls back to
 // the symmetric tree walk, which gives the same pair sets.
+// Both tests (r < h_i, r < h_j) are decided in FP32 from the 16-byte quantised
+// positions when the bound of QFrame (common.cuh) settles them, which it does
+// for all but ~1e-5 of the pairs; the rest load the FP64 positions.
 // Building the rows inside the pre-interaction's fused pass instead (pre split
 // into a smoothing-length launch and a fused launch, ballots and atomics in its
 // loop) was measured slower: shear 1 M pre + lists 7.1 ms against 4.8 + 1.7 ms.
@@ -42,7 +49,7 @@ __global__ void __launch_bounds__(LBLK) k_flist(DevParams P, DevState S, int n, 
                                                 const int* __restrict__ gcount, int gcap,
                                                 const double* __restrict__ rs, int* __restrict__ plist,
                                                 int* __restrict__ pcount, int* __restrict__ tcount, int pcap,
-                                                int* __restrict__ flags)
+                                                int* __restrict__ flags, DevTree Tr, double skin_delta)
 {
     constexpr int GPW = 32 / G;
     const int lane = threadIdx.x & (G - 1);
@@ -50,12 +57,24 @@ __global__ void __launch_bounds__(LBLK) k_flist(DevParams P, DevState S, int n, 
     const unsigned gmask = group_mask<G>();
     const long long warp = ((long long)blockIdx.x * LBLK + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * LBLK) >> 5;
+    const QFrame qf = qframe(P, Tr.geo);
+    const bool qok = *Tr.qbad == 0;
     for(long long wb = warp * GPW; wb < n; wb += nwarps * GPW) {
         const int i = (int)(wb + ((threadIdx.x & 31) / G));
         if(i >= n) continue;  // whole groups drop out together
         const double4 pi = S.pos[i];
         const double hi = S.vel[i].w;
-        if(!(hi <= rs[i]) && lane == 0) flags[0] = 1;  // the gather list may miss r < h_i
+        // the gather list may miss r < h_i; from a skin list (a superset) the
+        // pairs r < h_i are the gather list's when h_i < R_i - delta, and
+        // otherwise those that pass the exact membership test
+        const double ri = rs[i];
+        if(!(hi <= ri) && lane == 0) flags[0] = 1;
+        const bool exact = skin_delta > 0.0 && !(hi < ri - skin_delta);
+        // FP32 classification from the quantised positions (QFrame); the
+        // membership test needs the FP64 r^2 of every candidate
+        const bool quant = qok && !exact;
+        const int4 qi = Tr.qpos[i];
+        const float2 thi = qthresh(qf, hi);
         const int cnt = min(gcount[i], gcap);
         const int* li = glist + (size_t)i * (size_t)gcap;
         int* row = plist + (size_t)i * (size_t)pcap;
@@ -66,12 +85,37 @@ __global__ void __launch_bounds__(LBLK) k_flist(DevParams P, DevState S, int n, 
             int j = 0;
             if(k < cnt) {
                 j = __ldg(&li[k]);
-                const double4 pj = S.pos[j];
-                const Vec3d d = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
-                const double r = sqrt(abs2x(d));
-                if(r < hi) {
+                float dx = 0.f, dy = 0.f, dz = 0.f;
+                const bool near = quant && qdiff(qf, qi, __ldg(&Tr.qpos[j]), dx, dy, dz);
+                const float r2f = qr2(dx, dy, dz);
+                double r = -1.0;  // the FP64 distance, once formed
+                if(near && r2f >= thi.y) {
+                    own = false;
+                } else if(near && r2f < thi.x) {
                     own = true;
-                    if(!(r < __ldg(&S.vel[j].w))) {
+                } else {
+                    const double4 pj = S.pos[j];
+                    const Vec3d d = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
+                    const double r2 = abs2x(d);
+                    r = sqrt(r2);
+                    own = r < hi && (!exact || gather_member(P, Tr, pi.x, pi.y, pi.z, ri, skin_delta, j, r2));
+                }
+                if(own) {
+                    const double hj = __ldg(&S.vel[j].w);
+                    bool reach;
+                    const float2 thj = qthresh(qf, hj);
+                    if(r < 0.0 && near && r2f < thj.x) {
+                        reach = true;
+                    } else if(r < 0.0 && near && r2f >= thj.y) {
+                        reach = false;
+                    } else {
+                        if(r < 0.0) {
+                            const double4 pj = S.pos[j];
+                            r = sqrt(abs2x(rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z)));
+                        }
+                        reach = r < hj;
+                    }
+                    if(!reach) {
                         // j's own scan does not reach i: append i to j's row
                         const int t = atomicAdd(&tcount[j], 1);
                         if(t < pcap) plist[(size_t)j * (size_t)pcap + (pcap - 1 - t)] = i;
@@ -138,7 +182,8 @@ int build_force_lists(sphgpu_ctx* c)
     const long long gpb = LBLK / LG;
     const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>((n + gpb - 1) / gpb, 148LL * 8 * 4));
     k_flist<LG><<<grid, LBLK, 0, st>>>(c->dp, c->s, n, c->d_glist, c->d_gcount, (int)c->gcap, c->d_rsearch,
-                                       c->d_plist, c->d_pcount, c->d_tcount, (int)c->pcap, c->d_flist_flags);
+                                       c->d_plist, c->d_pcount, c->d_tcount, (int)c->pcap, c->d_flist_flags,
+                                       c->t, c->skin_valid ? c->skin_delta_now : 0.0);
     k_flist_finalize<<<grid_for(n, 256), 256, 0, st>>>(n, c->d_plist, c->d_pcount, c->d_tcount, (int)c->pcap,
                                                         c->prm.neighbor_number * 1000, c->d_flist_flags);
     SPHGPU_LAUNCH_CHECK(c, "force lists");

@@ -283,13 +283,25 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
             const int j = li[kk];
             const double4 pj = S.pos[j];
             const Vec3d d = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
-            const double r = sqrt(abs2x(d));
             const double4 vj = S.vel[j];
             const double hj = vj.w;
-            if(r >= (hi < hj ? hj : hi) || r == 0.0) continue;
+            double r, rinv;
+            if constexpr(f32) {
+                // the set predicate in FP64 (exact), the distance in FP32
+                const double r2 = abs2x(d);
+                if(!root_lt(r2, hi < hj ? hj : hi) || r2 == 0.0) continue;
+                const float r2f = (float)r2;
+                const float rif = rsqrtf(r2f);
+                r = (double)(r2f * rif);
+                rinv = (double)rif;
+                if(!(r > 0.0)) continue;  // r^2 below FP32's range: coincident for the force
+            } else {
+                r = sqrt(abs2x(d));
+                if(r >= (hi < hj ? hj : hi) || r == 0.0) continue;
+                rinv = 1.0 / r;
+            }
             ++n_pairs;
             const double4 tj = S.thermo[j];
-            const double rinv = 1.0 / r;
             const T rT = (T)r;
             const T rinvT = (T)rinv;
             const V3<T> rv{(T)d.x, (T)d.y, (T)d.z};

@@ -25,7 +25,10 @@
 // and not kept: walking each warp's path in segments, recording the opened
 // leaves' pairs, computing their terms with all 32 lanes and replaying the
 // segment to add every term in the reference's order (bit-identical, 190 ms:
-// the second pass over the nodes costs more than the divergence it removes).
+// the second pass over the nodes costs more than the divergence it removes);
+// lanes that park on an opened leaf until 5 / 10 / 16 lanes are parked and
+// then compute their next pairs together (169 / 225 / 286 ms: parked lanes
+// idle far longer than the divergent pairs take).
 #include <cuda_runtime.h>
 
 #include "context.cuh"

@@ -22,7 +22,11 @@
 // reference exactly; sums are taken in a different order than the
 // reference's distance-sorted loop, so results agree to rounding.
 // T = double: plain FP64 form.  T = float: pair arithmetic and sums in FP32
-// (mixed form); h, its Newton update and the predicates stay FP64.
+// (mixed form); h, its Newton update and the predicates stay FP64.  The mixed
+// form reads the 16-byte quantised positions (QFrame, common.cuh) first: the
+// smoothing-length sweeps decide r < h from them and take r from them, and the
+// fused pass skips the candidates they place surely outside h; the FP64 test
+// decides the few pairs within the bound of h.
 // Loading the next neighbour's position one iteration ahead as well (not only
 // its index) was measured slower: shear 1 M, 5.38 ms against 4.78 ms (FP64),
 // 4.29 against 3.67 ms (mixed); the extra live double4 adds spills.
@@ -68,10 +72,14 @@ constexpr int pre_min_blocks()
     return (sizeof(T) == sizeof(float) && TYPE != SPHGPU_GSPH && TYPE != SPHGPU_GDISPH) ? 4 : 3;
 }
 
+// skin_delta > 0: the lists are skin lists (supersets of the gather lists);
+// a particle whose h reaches R - skin_delta (R = its gather radius, the sml
+// the walk left) takes only exact members (gather_member).
 template <typename T, int G, int TYPE>
 __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevParams P, DevState S, int n, const int* __restrict__ list,
                                               const int* __restrict__ count, int cap, const double* __restrict__ dtp,
-                                              double* __restrict__ hvs, DevStatus* __restrict__ st)
+                                              double* __restrict__ hvs, DevStatus* __restrict__ st, DevTree Tr,
+                                              double skin_delta)
 {
     constexpr int GPW = 32 / G;
     const int lane = threadIdx.x & (G - 1);
@@ -85,7 +93,11 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
     const bool av_energy = disph && !(gdisph && P.balsara);
     double hv_min = DBL_MAX;
     unsigned nonconv = 0;
-    unsigned n_cand = 0, n_newton = 0, n_pairs = 0;  // work counters of this lane
+    unsigned n_cand = 0, n_newton = 0, n_pairs = 0, n_list = 0;  // work counters of this lane
+    // mixed form: candidates classified in FP32 from the quantised positions
+    constexpr bool f32 = sizeof(T) == sizeof(float);
+    const QFrame qf = qframe(P, Tr.geo);
+    const bool qok = *Tr.qbad == 0;
 
     for(long long wb = warp * GPW; wb < n; wb += nwarps * GPW) {
         const int i = (int)(wb + ((threadIdx.x & 31) / G));
@@ -96,6 +108,7 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
         const double4 vi = valid ? S.vel[i] : make_double4(0, 0, 0, 1);
         const double4 ti = valid ? S.thermo[i] : make_double4(1, 0, 0, 0);
         const double sml0 = vi.w;
+        const int4 qi = qok && valid ? Tr.qpos[i] : make_int4(0, 0, 0, 0);
 
         // ---- 1. smoothing length (src/pre_interaction.cpp:227-283,
         //         src/disph/d_pre_interaction.cpp:174-230)
@@ -108,6 +121,9 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
                 const double hb = h;
                 T d = 0, dd = 0;
                 const KernH<T> kh(P.kernel, (T)h);
+                const bool exact = skin_delta > 0.0 && !(h < sml0 - skin_delta);
+                const bool quant = qok && !exact;
+                const float2 th = qthresh(qf, h);
                 // the next candidate's index is fetched one iteration ahead,
                 // so the position load does not wait on the list load
                 int jn = lane < cnt ? __ldg(&li[lane]) : 0;
@@ -115,9 +131,38 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
                 for(int k = lane; k < cnt; k += G) {
                     const int jc = jn;
                     if(k + G < cnt) jn = __ldg(&li[k + G]);
+                    if constexpr(f32) {
+                        if(quant) {
+                            const int4 qj = __ldg(&Tr.qpos[jc]);
+                            float dx, dy, dz;
+                            const bool near = qdiff(qf, qi, qj, dx, dy, dz);
+                            const float r2f = qr2(dx, dy, dz);
+                            if(near && r2f >= th.y) continue;
+                            if(near && r2f < th.x) {
+                                ++n_newton;
+                                const T rT = r2f > 0.f ? r2f * rsqrtf(r2f) : 0.f;
+                                const T w = kh.w(rT);
+                                const T dh = kh.dhw(rT);
+                                if(disph) {
+                                    d += w;
+                                    dd += dh;
+                                } else {
+                                    const T mj = __int_as_float(qj.w);
+                                    d += mj * w;
+                                    dd += mj * dh;
+                                }
+                                continue;
+                            }
+                        }
+                    } else if(quant) {
+                        float dx, dy, dz;
+                        const bool near = qdiff(qf, qi, __ldg(&Tr.qpos[jc]), dx, dy, dz);
+                        if(near && qr2(dx, dy, dz) >= th.y) continue;
+                    }
                     const double4 pj = S.pos[jc];
+                    const double r2 = abs2x(rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z));
                     T rT;
-                    if(sweep_r(abs2x(rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z)), h, rT)) {
+                    if(sweep_r(r2, h, rT) && (!exact || gather_member(P, Tr, pi.x, pi.y, pi.z, sml0, skin_delta, jc, r2))) {
                         ++n_newton;
                         const T w = kh.w(rT);
                         const T dh = kh.dhw(rT);
@@ -155,15 +200,36 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
         int nn = 0;
         const bool need_av = !gsph && (P.balsara || P.td_av);
         const bool need_grad = (gsph || gdisph) && P.gsph2;
+        const bool exact = skin_delta > 0.0 && !(h < sml0 - skin_delta);
+        const bool quant = qok && !exact;
+        const float2 thf = qthresh(qf, h);
         int jn2 = lane < cnt ? __ldg(&li[lane]) : 0;
         n_cand += lane < cnt ? (unsigned)((cnt - lane + G - 1) / G) : 0u;
+        n_list += lane < cnt ? (unsigned)((cnt - lane + G - 1) / G) : 0u;
         for(int k = lane; k < cnt; k += G) {
             const int j = jn2;
             if(k + G < cnt) jn2 = __ldg(&li[k + G]);
+            // candidates surely outside h need no FP64 position
+            if(quant) {
+                float dx, dy, dz;
+                const bool near = qdiff(qf, qi, __ldg(&Tr.qpos[j]), dx, dy, dz);
+                if(near && qr2(dx, dy, dz) >= thf.y) continue;
+            }
             const double4 pj = S.pos[j];
             const Vec3d dv = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
+            const double r2 = abs2x(dv);
             double r, rinv;
-            if(!pair_within(abs2x(dv), h, r, rinv)) continue;
+            if constexpr(sizeof(T) == sizeof(float)) {
+                // the set predicate in FP64, the distance in FP32 (mixed form)
+                if(!root_lt(r2, h)) continue;
+                const float r2f = (float)r2;
+                const float rif = r2f > 0.f ? rsqrtf(r2f) : 0.f;
+                r = (double)(r2f * rif);
+                rinv = (double)rif;
+            } else {
+                if(!pair_within(r2, h, r, rinv)) continue;
+            }
+            if(exact && !gather_member(P, Tr, pi.x, pi.y, pi.z, sml0, skin_delta, j, r2)) continue;
             ++nn;
             const double4 vj = S.vel[j];
             const double4 tj = S.thermo[j];
@@ -350,6 +416,7 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
     block_count(&st->pre_cand, n_cand);
     block_count(&st->pre_newton_pairs, n_newton);
     block_count(&st->pre_pairs, n_pairs);
+    block_count(&st->pre_list, n_list);
 }
 
 // PreInteraction::initial_smoothing (src/pre_interaction.cpp:171-215):
@@ -397,19 +464,20 @@ template <typename T>
 void launch_pre(sphgpu_ctx* c)
 {
     const unsigned grid = pre_grid(c->n);
+    const double sd = c->skin_valid ? c->skin_delta_now : 0.0;
     const int type = c->prm.sph_type;
     if(type == SPHGPU_DISPH) {
         k_pre<T, GROUP, SPHGPU_DISPH><<<grid, PBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_glist, c->d_gcount,
-                                                                    (int)c->gcap, c->d_dt, c->d_hvs, c->d_status);
+                                                                    (int)c->gcap, c->d_dt, c->d_hvs, c->d_status, c->t, sd);
     } else if(type == SPHGPU_GSPH) {
         k_pre<T, GROUP, SPHGPU_GSPH><<<grid, PBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_glist, c->d_gcount,
-                                                                   (int)c->gcap, c->d_dt, c->d_hvs, c->d_status);
+                                                                   (int)c->gcap, c->d_dt, c->d_hvs, c->d_status, c->t, sd);
     } else if(type == SPHGPU_GDISPH) {
         k_pre<T, GROUP, SPHGPU_GDISPH><<<grid, PBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_glist, c->d_gcount,
-                                                                     (int)c->gcap, c->d_dt, c->d_hvs, c->d_status);
+                                                                     (int)c->gcap, c->d_dt, c->d_hvs, c->d_status, c->t, sd);
     } else {
         k_pre<T, GROUP, SPHGPU_SSPH><<<grid, PBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_glist, c->d_gcount,
-                                                                   (int)c->gcap, c->d_dt, c->d_hvs, c->d_status);
+                                                                   (int)c->gcap, c->d_dt, c->d_hvs, c->d_status, c->t, sd);
     }
 }
 
@@ -437,7 +505,7 @@ int pre_interaction(sphgpu_ctx* c)
         stage_end(c, SPHGPU_T_PRE, 1);
         c->first_pre = false;
     }
-    rc_walk = gather_walk(c, true, c->dp.ratio);
+    rc_walk = gather_lists(c, c->dp.ratio);
     if(rc_walk < 0) return rc_walk;
     int rcs = save_gather_radius(c);
     if(rcs < 0) return rcs;

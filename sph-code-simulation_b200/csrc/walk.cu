@@ -33,6 +33,8 @@
 // longer than the capacity is counted but not stored; the host grows the
 // buffer and re-runs (status.overflow).  More than neighbor_number * 1000
 // entries is the reference's fatal overflow (src/bhtree.cpp:129-135).
+#include <algorithm>
+#include <cmath>
 #include <cstddef>
 #include <cuda_runtime.h>
 
@@ -104,10 +106,21 @@ __device__ __forceinline__ int walk_lanes(const DevParams& P, const DevState& S,
     return cnt;
 }
 
+// Skin (Verlet) gather lists: the gather walk runs with radius factor x the
+// guessed radius and records each particle's walk radius and position, so
+// later steps can reuse the lists while every particle's true gather sphere
+// stays inside its skin sphere (skin_check).  factor = 1, r = x = null: the
+// reference's exact lists.
+struct SkinOut {
+    double factor;
+    double* r;
+    double4* x;
+};
+
 template <bool IJ>
 __global__ void __launch_bounds__(WBLK) k_walk(DevParams P, DevState S, DevTree T, int n, int cap,
                                                int* __restrict__ list, int* __restrict__ count,
-                                               DevStatus* __restrict__ st, int guess, double ratio)
+                                               DevStatus* __restrict__ st, int guess, double ratio, SkinOut sk)
 {
     const int i = blockIdx.x * WBLK + threadIdx.x;
     const bool valid = i < n;
@@ -121,8 +134,13 @@ __global__ void __launch_bounds__(WBLK) k_walk(DevParams P, DevState S, DevTree 
             // h guess from the previous density (src/pre_interaction.cpp:61-64)
             constexpr double A = 4.0 * 3.14159265358979323846 / 3.0;
             const double dens = S.thermo[i].x;
-            hi = pow(P.nngb * p.w / (dens * A), 1.0 / 3) * ratio;
-            S.vel[i].w = hi;
+            const double g = pow(P.nngb * p.w / (dens * A), 1.0 / 3) * ratio;
+            S.vel[i].w = g;
+            hi = g * sk.factor;
+            if(sk.r) {
+                sk.r[i] = hi;
+                sk.x[i] = p;
+            }
         } else {
             hi = S.vel[i].w;
         }
@@ -191,7 +209,8 @@ __device__ __forceinline__ bool box_pass(const DevParams& P, const DevTree& T, i
 template <bool IJ>
 __global__ void __launch_bounds__(GW_WARPS * 32) k_walk_group(DevParams P, DevState S, DevTree T, int n, int cap,
                                                              int* __restrict__ list, int* __restrict__ count,
-                                                             DevStatus* __restrict__ st, int guess, double ratio)
+                                                             DevStatus* __restrict__ st, int guess, double ratio,
+                                                             SkinOut sk)
 {
     __shared__ int s_stack[GW_WARPS][GW_STACK];
     __shared__ int s_queue[GW_WARPS][GW_QUEUE];
@@ -214,8 +233,13 @@ __global__ void __launch_bounds__(GW_WARPS * 32) k_walk_group(DevParams P, DevSt
         zi = p.z;
         if(guess) {
             constexpr double A = 4.0 * 3.14159265358979323846 / 3.0;
-            hi = pow(P.nngb * p.w / (S.thermo[i].x * A), 1.0 / 3) * ratio;
-            S.vel[i].w = hi;
+            const double g = pow(P.nngb * p.w / (S.thermo[i].x * A), 1.0 / 3) * ratio;
+            S.vel[i].w = g;
+            hi = g * sk.factor;
+            if(sk.r) {
+                sk.r[i] = hi;
+                sk.x[i] = p;
+            }
         } else {
             hi = S.vel[i].w;
         }
@@ -566,7 +590,8 @@ __global__ void k_fill_by_id(int n, int cap, const int* __restrict__ id, const i
     for(int k = 0; k < c; ++k) out[b + k] = id[list[(size_t)i * cap + k]];
 }
 
-int run_walk(sphgpu_ctx* c, int which, bool guess, double ratio, bool exhaustive, int is_ij, int* launches)
+int run_walk(sphgpu_ctx* c, int which, bool guess, double ratio, bool exhaustive, int is_ij, int* launches,
+             SkinOut sk = SkinOut{1.0, nullptr, nullptr})
 {
     cudaStream_t st = c->stream;
     const int n = c->n;
@@ -584,17 +609,17 @@ int run_walk(sphgpu_ctx* c, int which, bool guess, double ratio, bool exhaustive
             const unsigned grid = grid_for(n, GW_WARPS * 32);
             if(which == 0) {
                 k_walk_group<false><<<grid, GW_WARPS * 32, 0, st>>>(c->dp, c->s, c->t, n, (int)cap, list, count,
-                                                                   c->d_status, guess ? 1 : 0, ratio);
+                                                                   c->d_status, guess ? 1 : 0, ratio, sk);
             } else {
                 k_walk_group<true><<<grid, GW_WARPS * 32, 0, st>>>(c->dp, c->s, c->t, n, (int)cap, list, count,
-                                                                  c->d_status, 0, 1.0);
+                                                                  c->d_status, 0, 1.0, SkinOut{1.0, nullptr, nullptr});
             }
         } else if(which == 0) {
             k_walk<false><<<grid_for(n, WBLK), WBLK, 0, st>>>(c->dp, c->s, c->t, n, (int)cap, list, count,
-                                                            c->d_status, guess ? 1 : 0, ratio);
+                                                            c->d_status, guess ? 1 : 0, ratio, sk);
         } else {
             k_walk<true><<<grid_for(n, WBLK), WBLK, 0, st>>>(c->dp, c->s, c->t, n, (int)cap, list, count,
-                                                           c->d_status, 0, 1.0);
+                                                           c->d_status, 0, 1.0, SkinOut{1.0, nullptr, nullptr});
         }
         SPHGPU_LAUNCH_CHECK(c, "neighbour walk");
         // the first seven status words: the walk's own and the pass guard of
@@ -636,10 +661,233 @@ int run_walk(sphgpu_ctx* c, int which, bool guess, double ratio, bool exhaustive
 int gather_walk(sphgpu_ctx* c, bool compute_guess, double ratio)
 {
     if(!c->have_tree) return fail(c, SPHGPU_ERR_STATE, "neighbour search before tree make");
+    c->skin_valid = false;  // the exact lists replace any skin lists
     stage_begin(c, SPHGPU_T_GATHER_WALK);
     int launches = 0;
     const int rc = run_walk(c, 0, compute_guess, ratio, false, 0, &launches);
     stage_end(c, SPHGPU_T_GATHER_WALK, launches);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Skin lists.  The step's true gather list of particle i is
+//   { j : r_ij < R_i, box tests on the path }, R_i = ratio * the h guess,
+// and every such j satisfies r_ij < R_i - delta or lies in the band replayed
+// by box tests.  A list built with radius F_i >= R_i at positions x^b holds
+// every j with |x_i^b - x_j^b| < F_i - delta.  Since
+//   |x_i^b - x_j^b| <= r_ij + d_i + d_j  (d = displacement since the build,
+//   minimum image),
+// it holds the step's true list when R_i + d_i + d_max < F_i - delta for
+// every i (d_max = the largest displacement).  Consumers take from a skin list
+// exactly the members of the true list: pairs with r < h for h < R - delta
+// need no other test (they are members); PreInteraction tests membership
+// exactly for a particle whose h reaches R - delta, and the force-list build
+// falls back to the symmetric walk for it.
+
+namespace {
+
+// The h guess into sml (the walk's expression, bit for bit), and the largest
+// displacement since the build (rounded up).
+__global__ void k_skin_guess(DevParams P, DevState S, int n, double ratio, const double4* __restrict__ xb,
+                             double* __restrict__ dmax)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double d = 0.0;
+    if(i < n) {
+        const double4 p = S.pos[i];
+        constexpr double A = 4.0 * 3.14159265358979323846 / 3.0;
+        S.vel[i].w = pow(P.nngb * p.w / (S.thermo[i].x * A), 1.0 / 3) * ratio;
+        const double4 b = xb[i];
+        const Vec3d v = rij(P, p.x, p.y, p.z, b.x, b.y, b.z);
+        d = sqrt(v.x * v.x + v.y * v.y + v.z * v.z) * (1.0 + 1e-12);
+    }
+    d = warp_max_pos(d);
+    if((threadIdx.x & 31) == 0 && d > 0.0) atomic_max_pos(dmax, d);
+}
+
+__global__ void k_skin_check(DevParams P, DevState S, int n, const double* __restrict__ fr,
+                             const double4* __restrict__ xb, const double* __restrict__ dmax, double delta,
+                             int* __restrict__ bad)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const double4 p = S.pos[i];
+    const double4 b = xb[i];
+    const Vec3d v = rij(P, p.x, p.y, p.z, b.x, b.y, b.z);
+    const double d = sqrt(v.x * v.x + v.y * v.y + v.z * v.z) * (1.0 + 1e-12);
+    const double need = (S.vel[i].w + d + *dmax) * (1.0 + 1e-12) + 2.0 * delta;
+    if(!(need < fr[i])) *bad = 1;
+}
+
+// Lists, counts, radii and build positions of the previous particle order
+// moved to the order of the new tree (particle q now at p = new_of_old[q]).
+__global__ void k_skin_new_of_old(const uint32_t* __restrict__ src, int n, int* __restrict__ new_of_old)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p < n) new_of_old[src[p]] = p;
+}
+
+__global__ void k_skin_permute(const uint32_t* __restrict__ src, int n, int cap, const int* __restrict__ new_of_old,
+                               const int* __restrict__ list, const int* __restrict__ count, const double* __restrict__ fr,
+                               const double4* __restrict__ xb, int* __restrict__ list2, int* __restrict__ count2,
+                               double* __restrict__ fr2, double4* __restrict__ xb2)
+{
+    // one warp per row
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if(w >= n) return;
+    const int p = (int)w;
+    const int q = (int)src[p];
+    const int cnt = min(count[q], cap);
+    const int* a = list + (size_t)q * (size_t)cap;
+    int* b = list2 + (size_t)p * (size_t)cap;
+    if((cap & 3) == 0) {
+        // rows start on 16 bytes: four entries per lane and load, four
+        // independent gathers in flight (entries past cnt are copied as is)
+        const int4* a4 = reinterpret_cast<const int4*>(a);
+        int4* b4 = reinterpret_cast<int4*>(b);
+        for(int e = lane; 4 * e < cnt; e += 32) {
+            int4 v = __ldg(&a4[e]);
+            const int k = 4 * e;
+            v.x = __ldg(&new_of_old[v.x]);
+            if(k + 1 < cnt) v.y = __ldg(&new_of_old[v.y]);
+            if(k + 2 < cnt) v.z = __ldg(&new_of_old[v.z]);
+            if(k + 3 < cnt) v.w = __ldg(&new_of_old[v.w]);
+            b4[e] = v;
+        }
+    } else {
+        for(int e = lane; e < cnt; e += 32) b[e] = __ldg(&new_of_old[__ldg(&a[e])]);
+    }
+    if(lane == 0) {
+        count2[p] = cnt;
+        fr2[p] = fr[q];
+        xb2[p] = xb[q];
+    }
+}
+
+}  // namespace
+
+// The walk's safety margin (1e-12 of the domain scale) for the current tree,
+// from its root box; 1e300 (no reuse) if it cannot be read.
+double skin_delta(sphgpu_ctx* c)
+{
+    double4 root;
+    if(cudaMemcpyAsync(&root, c->t.geo, sizeof(double4), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+       cudaStreamSynchronize(c->stream) != cudaSuccess)
+        return 1e300;
+    return 1e-12 * (std::max(std::fabs(root.x), std::max(std::fabs(root.y), std::fabs(root.z))) + root.w);
+}
+
+int skin_alloc(sphgpu_ctx* c)
+{
+    const int64_t want = (int64_t)c->n * c->gcap;
+    if(c->skin_n == c->n && c->skin_cap == c->gcap && c->d_skin) return SPHGPU_OK;
+    if(c->d_skin) {
+        SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+        SPHGPU_CUDA(c, cudaFree(c->d_skin));
+        c->d_skin = nullptr;
+    }
+    if(c->d_glist_alt) {
+        SPHGPU_CUDA(c, cudaFree(c->d_glist_alt));
+        c->d_glist_alt = nullptr;
+    }
+    // the second list buffer is an allocation of its own: it trades places
+    // with d_glist at every permutation
+    SPHGPU_CUDA(c, cudaMalloc(&c->d_glist_alt, std::max<size_t>(4 * (size_t)want, 4)));
+    const size_t n = (size_t)c->n;
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t bytes = al(4 * n) + 2 * al(8 * n) + 2 * al(32 * n) + al(4 * n) + 256;
+    SPHGPU_CUDA(c, cudaMalloc(&c->d_skin, bytes));
+    char* b = static_cast<char*>(c->d_skin);
+    size_t off = 0;
+    auto take = [&](size_t sz) {
+        char* q = b + off;
+        off += al(sz);
+        return q;
+    };
+    c->d_gcount_alt = reinterpret_cast<int*>(take(4 * n));
+    c->d_skin_r = reinterpret_cast<double*>(take(8 * n));
+    c->d_skin_r_alt = reinterpret_cast<double*>(take(8 * n));
+    c->d_skin_x = reinterpret_cast<double4*>(take(32 * n));
+    c->d_skin_x_alt = reinterpret_cast<double4*>(take(32 * n));
+    c->d_skin_new = reinterpret_cast<int*>(take(4 * n));
+    c->d_skin_scal = reinterpret_cast<double*>(take(16));
+    c->skin_n = c->n;
+    c->skin_cap = c->gcap;
+    c->skin_valid = false;
+    return SPHGPU_OK;
+}
+
+int skin_permute(sphgpu_ctx* c, const uint32_t* src)
+{
+    if(!c->skin_valid) return SPHGPU_OK;
+    if(c->skin_n != c->n || c->skin_cap != c->gcap) {
+        c->skin_valid = false;
+        return SPHGPU_OK;
+    }
+    const int n = c->n;
+    k_skin_new_of_old<<<grid_for(n, 256), 256, 0, c->stream>>>(src, n, c->d_skin_new);
+    k_skin_permute<<<grid_for((long long)n * 32, 256), 256, 0, c->stream>>>(
+        src, n, (int)c->gcap, c->d_skin_new, c->d_glist, c->d_gcount, c->d_skin_r, c->d_skin_x, c->d_glist_alt,
+        c->d_gcount_alt, c->d_skin_r_alt, c->d_skin_x_alt);
+    SPHGPU_LAUNCH_CHECK(c, "skin list permutation");
+    std::swap(c->d_glist, c->d_glist_alt);
+    SPHGPU_CUDA(c, cudaMemcpyAsync(c->d_gcount, c->d_gcount_alt, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice,
+                                   c->stream));
+    std::swap(c->d_skin_r, c->d_skin_r_alt);
+    std::swap(c->d_skin_x, c->d_skin_x_alt);
+    c->stage_launch[SPHGPU_T_TREE] += 2;
+    c->launches += 2;
+    return SPHGPU_OK;
+}
+
+int gather_lists(sphgpu_ctx* c, double ratio)
+{
+    if(!c->have_tree) return fail(c, SPHGPU_ERR_STATE, "neighbour search before tree make");
+    const double skin = c->prm.gather_skin;
+    if(!(skin > 0.0) || c->walk_mode != 0) return gather_walk(c, true, ratio);
+    cudaStream_t st = c->stream;
+    const int n = c->n;
+    c->skin_delta_now = skin_delta(c);
+    if(!(c->skin_delta_now < 1e299)) return gather_walk(c, true, ratio);
+    if(c->skin_valid) {
+        stage_begin(c, SPHGPU_T_GATHER_WALK);
+        double* dmax = c->d_skin_scal;
+        int* bad = reinterpret_cast<int*>(c->d_skin_scal + 1);
+        SPHGPU_CUDA(c, cudaMemsetAsync(c->d_skin_scal, 0, 16, st));
+        k_skin_guess<<<grid_for(n, 256), 256, 0, st>>>(c->dp, c->s, n, ratio, c->d_skin_x, dmax);
+        k_skin_check<<<grid_for(n, 256), 256, 0, st>>>(c->dp, c->s, n, c->d_skin_r, c->d_skin_x, dmax,
+                                                        c->skin_delta_now, bad);
+        SPHGPU_LAUNCH_CHECK(c, "skin check");
+        int hbad = 1;
+        SPHGPU_CUDA(c, cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+        SPHGPU_CUDA(c, cudaStreamSynchronize(st));
+        stage_end(c, SPHGPU_T_GATHER_WALK, 2);
+        if(!hbad) {
+            ++c->skin_reuses;
+            return SPHGPU_OK;
+        }
+    }
+    // build: the walk at radius (1 + skin) R, recording radii and positions
+    int rc = ensure_list_capacity(c, 0, c->gcap);
+    if(rc < 0) return rc;
+    rc = skin_alloc(c);
+    if(rc < 0) return rc;
+    c->skin_valid = false;
+    stage_begin(c, SPHGPU_T_GATHER_WALK);
+    int launches = 0;
+    rc = run_walk(c, 0, true, ratio, false, 0, &launches, SkinOut{1.0 + skin, c->d_skin_r, c->d_skin_x});
+    stage_end(c, SPHGPU_T_GATHER_WALK, launches);
+    if(rc == SPHGPU_ERR_NEIGHBOR_OVERFLOW) return gather_walk(c, true, ratio);  // decided on the exact lists
+    if(rc < 0) return rc;
+    if(c->skin_n != c->n || c->skin_cap != c->gcap) {
+        // the walk grew the lists past the skin buffers: take exact lists for
+        // this step (consumers treat lists as skin lists only while
+        // skin_valid); the buffers follow at the next build
+        return gather_walk(c, true, ratio);
+    }
+    c->skin_valid = true;
+    ++c->skin_builds;
     return rc;
 }
 

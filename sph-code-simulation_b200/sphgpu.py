@@ -90,8 +90,9 @@ class Counters(C.Structure):
         "newton_nonconverged", "riemann_solves", "riemann_iterations", "riemann_fallbacks",
         "gather_capacity", "max_gather", "max_pair", "node_count", "retries", "walk_group_warps",
         "walk_split_warps", "walk_fallbacks", "mlp_guesses", "force_list_builds", "pre_candidates",
-        "pre_newton_pairs", "pre_pairs", "force_candidates", "force_pairs", "gravity_nodes",
-        "gravity_monopoles", "gravity_leaf_pairs", "mixed_rechecks")]
+        "pre_newton_pairs", "pre_pairs", "pre_list_entries", "force_candidates", "force_pairs", "gravity_nodes",
+        "gravity_monopoles", "gravity_leaf_pairs", "mixed_rechecks", "skin_builds",
+        "skin_reuses")]
 
 
 _lib = None

@@ -50,6 +50,7 @@ class Params(C.Structure):
         ("mlp_max_newton", C.c_int32), ("sr_2nd_order", C.c_int32), ("tree_root_origin", C.c_int32),
         ("sr_c_speed", C.c_double), ("sr_c_shock", C.c_double), ("sr_c_cd", C.c_double), ("sr_eta", C.c_double),
         ("sr_c_smooth", C.c_double), ("mixed_acc_tol", C.c_double), ("riemann_tol", C.c_double),
+        ("gather_skin", C.c_double),
     ]
 
     def copy(self) -> "Params":
@@ -72,7 +73,7 @@ DEFAULTS = dict(
     leaf_particle_num=1, periodic=0, use_gravity=0, gsph_2nd_order=1, g_constant=1.0, theta=0.5,
     riemann_solver=RIEMANN_HLL, precision=FP64, riemann_guess=GUESS_NONE, mlp_max_newton=4,
     sr_2nd_order=1, tree_root_origin=1, sr_c_speed=1.0, sr_c_shock=3.0, sr_c_cd=1.0, sr_eta=1.0,
-    sr_c_smooth=2.0, mixed_acc_tol=0.0, riemann_tol=1e-6,
+    sr_c_smooth=2.0, mixed_acc_tol=0.0, riemann_tol=1e-6, gather_skin=0.02,
 )
 
 

@@ -65,6 +65,12 @@ oracle/_ref/libsphref*.so, driven by oracle/ref_harness.cpp):
                      faces and one coincident pair, iterative and fixed h,
                      Balsara off, first-order gsph with the iterative solver.
                      Inputs are rebuilt from the sweep_* functions below.
+  evrard_disph_8.78M_reference.json
+                     The full 256^3 disph Evrard sphere (8,783,848 particles)
+                     at cflSound 0.05 / cflForce 0.025, step by step until the
+                     reference's own state turns non-finite: dt, time, K, U, W,
+                     the smallest u, and the first bad particles' ids
+                     (`python tests/golden/make_golden.py evrard_big`, slow).
   lists_<cfg>.npz    Distance-sorted neighbour lists (CSR) from
                      BHTree::neighbor_search and from exhaustive_search
                      (gather and is_ij) at the state after initialize.
@@ -506,8 +512,44 @@ def main():
     sweep_golden()
 
 
+def evrard_big_reference(steps=20, threads=0):
+    """The compiled reference on the full 256^3 disph Evrard sphere
+    (8,783,848 particles, the default benchmark workload's physics) at
+    cflSound 0.05 / cflForce 0.025, step by step until its state turns
+    non-finite: dt, time, K, U, W, the smallest internal energy, and the
+    caller ids of the first particles with u <= 0 or a non-finite sound speed
+    or position.  Slow: about 4.5 minutes per step on 6 host cores
+    (python tests/golden/make_golden.py evrard_big)."""
+    import json
+    import time
+    p = G.config_params("evrard_disph", cfl_sound=0.05, cfl_force=0.025)
+    f = G.sample_evrard(256)
+    threads = threads or max(2, os.cpu_count() - 2)
+    ref = O.Reference(p, f, threads=threads)
+    t0 = time.time()
+    ref.initialize()
+    rec = {"n": len(f["pos_x"]), "cfl": [0.05, 0.025], "threads": threads, "init_s": time.time() - t0,
+           "steps": []}
+    for s in range(steps):
+        t1 = time.time()
+        ref.integrate()
+        st = ref.download(["ene", "sound", "pos_x", "dens"])
+        bad = np.where(~np.isfinite(st["sound"]) | ~np.isfinite(st["pos_x"]) | (st["ene"] <= 0))[0]
+        k, u, w, _ = ref.energies()
+        rec["steps"].append({"step": s + 1, "time": ref.time, "dt": ref.dt, "K": k, "U": u, "W": w,
+                             "umin": float(np.nanmin(st["ene"])), "rhomax": float(np.nanmax(st["dens"])),
+                             "nbad": int(bad.size), "bad": bad[:32].tolist(), "sec": time.time() - t1})
+        with open(os.path.join(OUT, "evrard_disph_8.78M_reference.json"), "w") as fh:
+            json.dump(rec, fh, indent=1)
+        if bad.size:
+            break
+
+
 if __name__ == "__main__":
-    if sys.argv[1:] == ["edge"]:
+    if sys.argv[1:] == ["evrard_big"]:
+        O.build(reference=True)
+        evrard_big_reference()
+    elif sys.argv[1:] == ["edge"]:
         O.build(reference=True)
         for name in EDGE:
             edge_steps(name)

@@ -39,7 +39,7 @@ def test_params_struct_layout(G, tmp_path):
     """The ctypes mirror has the C compiler's offsets for every field."""
     import ctypes
     import subprocess
-    assert ctypes.sizeof(G.Params) == 256
+    assert ctypes.sizeof(G.Params) == 264
     assert G.Params.sr_2nd_order.offset == 192 and G.Params.tree_root_origin.offset == 196
     assert G.Params.sr_c_speed.offset == 200
     names = [f[0] for f in G.Params._fields_]

@@ -1,0 +1,81 @@
+"""Skin (Verlet) gather lists (gather_skin, walk.cu): the lists of one walk at
+(1 + skin) times the gather radius are reused, moved to each new tree's
+particle order, while every gather sphere stays inside its list's sphere; the
+consumers take exactly the reference's list members from them.  The steps
+must equal those with a fresh exact walk every step: the same neighbour
+counts and states to rounding (sums over the same sets in another order),
+and the same tree and gravity bit for bit."""
+import numpy as np
+import pytest
+
+import ics
+import sphparams as SP
+from test_gpu_parity import _close
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "evrard_disph": lambda: (SP.config_params("evrard_disph", cfl_sound=0.05, cfl_force=0.025), ics.evrard(24)),
+    "shear_disph": lambda: (SP.config_params("shear_disph"), ics.shear_layer(0.02)),
+    "tube_gsph": lambda: (SP.config_params("tube_gsph", range_min=(-0.5, 0.0, 0.0), range_max=(0.5, 0.1, 0.1)),
+                          ics.shock_tube(0.01, ly=0.1)),
+    "evrard_ssph_fixed_h": lambda: (SP.config_params("evrard_ssph", iterative_sml=0), ics.evrard(16)),
+}
+
+
+def _run(G, p, f, skin, steps):
+    q = p.copy()
+    q.gather_skin = skin
+    with G.Simulation(q) as sim:
+        sim.upload(f)
+        sim.initialize()
+        sim.reset_counters()
+        out = []
+        for _ in range(steps):
+            sim.integrate()
+            out.append(sim.download())
+        return out, sim.counters()
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+@pytest.mark.parametrize("skin", [0.05, 0.002])
+def test_skin_lists_match_exact_walk(gpu, case, skin):
+    p, f = CASES[case]()
+    ref, c0 = _run(gpu, p, f, 0.0, 6)
+    out, c1 = _run(gpu, p, f, skin, 6)
+    assert c0["skin_reuses"] == 0
+    if skin >= 0.05:
+        assert c1["skin_reuses"] >= 4, c1     # most steps reuse the lists
+    assert c1["skin_builds"] + c1["skin_reuses"] == 6
+    for s, (a, b) in enumerate(zip(out, ref)):
+        np.testing.assert_array_equal(a["neighbor"], b["neighbor"], err_msg=f"step {s + 1}")
+        for fld in ("dens", "sml", "pres", "ene"):
+            _close(a[fld], b[fld], f"step {s + 1} {fld}", median=1e-12, p999=1e-9, worst=1e-6)
+        amax = max(np.max(np.abs(b[f"acc_{x}"])) for x in "xyz")
+        for x in "xyz":
+            _close(a[f"acc_{x}"], b[f"acc_{x}"], f"step {s + 1} acc_{x}", scale=amax, median=1e-12, p999=1e-9,
+                   worst=1e-6)
+
+
+def test_skin_lists_export_exact_lists(gpu):
+    """sphgpu_neighbor_search still returns the reference's lists (a fresh
+    exact walk) after steps that reused skin lists."""
+    p, f = CASES["shear_disph"]()
+    with gpu.Simulation(p) as sim:
+        sim.upload(f)
+        sim.initialize()
+        for _ in range(3):
+            sim.integrate()
+        assert sim.counters()["skin_reuses"] >= 1
+        st = sim.download()
+        off, ids = sim.neighbor_search(is_ij=False)
+    q = p.copy()
+    q.gather_skin = 0.0
+    with gpu.Simulation(q) as sim:
+        sim.upload({k: v for k, v in st.items() if not k.startswith("sr_")})
+        sim.tree_make()
+        off2, ids2 = sim.neighbor_search(is_ij=False)
+    np.testing.assert_array_equal(off, off2)
+    n = len(off) - 1
+    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(off))
+    np.testing.assert_array_equal(np.sort(rows * n + ids), np.sort(rows * n + ids2))
