@@ -133,7 +133,8 @@ typedef struct sphgpu_params {
      * times the gather radius and later steps reuse them, moved to each new
      * tree's particle order, while every particle's gather sphere stays
      * inside its list's sphere (displacements are tracked); the consumers
-     * take exactly the reference's list members from them.  0 = a fresh
+     * take exactly the reference's list members from them.  Two builds in
+     * a row that are never reused pause the skin for 32 steps.  0 = a fresh
      * exact walk every step.  (0.02)                                      */
     double  gather_skin;
 } sphgpu_params;

@@ -215,8 +215,7 @@ int alloc_all(sphgpu_ctx* c, int n)
        || (rc = dalloc(c, c->t.link, nc)) || (rc = dalloc(c, c->t.parent, nc)) || (rc = dalloc(c, c->t.nchild, nc))
        || (rc = dalloc(c, c->t.child, 8 * (size_t)nc))
        || (rc = dalloc(c, c->t.counter, nc)) || (rc = dalloc(c, c->t.nnodes, 4))
-       || (rc = dalloc(c, c->t.leaf_of, n)) || (rc = dalloc(c, c->t.pks, n)) || (rc = dalloc(c, c->t.qpos, n))
-       || (rc = dalloc(c, c->t.qbad, 1)))
+       || (rc = dalloc(c, c->t.leaf_of, n)) || (rc = dalloc(c, c->t.pks, n)))
         return rc;
     if((rc = dalloc(c, c->d_root, 1)) || (rc = dalloc(c, c->d_bbox_part, 6 * 1024)) || (rc = dalloc(c, c->d_keys, n))
        || (rc = dalloc(c, c->d_keys_alt, n)) || (rc = dalloc(c, c->d_vals, n)) || (rc = dalloc(c, c->d_vals_alt, n))
@@ -580,6 +579,7 @@ int sphgpu_upload(sphgpu_ctx* c, int64_t n, const double* const* fields)
     c->flist_ready = false;
     c->first_pre = true;
     c->skin_valid = false;
+    c->skin_since_build = c->skin_idle = c->skin_off = 0;
     c->time = 0.0;
     return SPHGPU_OK;
 }

@@ -80,8 +80,6 @@ struct DevTree {
     int* nnodes;     // device scalar: total node count (root included)
     int* leaf_of;    // per particle (tree order): the leaf holding it
     double* pks;     // per particle: kernel_size of its leaf (set_kernel)
-    int4* qpos;      // per particle: quantised position and FP32 mass (QFrame)
-    int* qbad;       // device scalar: nonzero = a particle lies outside the QFrame
 };
 
 // Packed status words read back by the host after a module.
@@ -242,85 +240,6 @@ __device__ __forceinline__ bool root_lt(double r2, double h)
     if(r2 < h2 * (1.0 - 0x1p-40)) return true;
     if(r2 > h2 * (1.0 + 0x1p-40)) return false;
     return sqrt(r2) < h;
-}
-
-// ---------------------------------------------------------------------------
-// Quantised positions: 16-byte records {qx, qy, qz, mass as float bits} that
-// the pair loops classify most candidates from in FP32, loading the 32-byte
-// FP64 position only for the few whose answer the FP32 bound leaves open.
-// Per axis q = round((x - lo) s) as a 32-bit integer; differences are taken in
-// wrapping integer arithmetic, so on a periodic axis (s = 2^32 / L) they are
-// the minimum image, and on an open axis (the root box, a little widened,
-// mapped onto [0, 2^31)) they never overflow.  A quantum is 2^-31 of the box
-// (2^-32 periodic); the mixed form's smoothing-length sweeps take their
-// distances from these records too, every other pair term from FP64
-// positions.  Error of the FP32
-// difference d' = float(q_i - q_j) * float(1 / s) against the exact difference
-// d, per axis: |d' - d| <= 1.01 / s + 3.1 * 2^-24 |d| (two rounding halves of
-// q, the conversion, 1 / s and the product in FP32); the FP32 sum of squares
-// adds 3 * 2^-24.  So with a = 2 / s:
-//   r2f <  ((h - a)(1 - 2^-20))^2  (rounded down to FP32)  =>  |d| < h (1 - 2^-21)
-//   r2f >= ((h + a)(1 + 2^-20))^2  (rounded up)            =>  |d| > h (1 + 2^-21)
-// and the reference's FP64 r (sqrt of the rounded r^2, ~3 * 2^-53 |d| from
-// |d|) then compares with h the same way.  Everything between, and every
-// pair with an axis difference of 2^30 quanta or more (where a periodic
-// axis's image could differ from the reference's choice), takes the FP64
-// test.  DevTree::qbad (a particle outside the frame) sends every pair to the
-// FP64 test.
-struct QFrame {
-    double lo[3], s[3];
-    float inv[3];
-    double a;  // 2 / min(s): the absolute part of the bound
-};
-
-__device__ __forceinline__ QFrame qframe(const DevParams& P, const double4* __restrict__ geo)
-{
-    QFrame f;
-    if(P.periodic) {
-        for(int k = 0; k < 3; ++k) {
-            f.lo[k] = P.lo[k];
-            f.s[k] = 0x1p32 / P.range[k];
-        }
-    } else {
-        // the root box widened by 2^-8 of its edge, mapped onto [0, 2^31)
-        const double4 g = geo[0];
-        const double span = (g.w > 0.0 ? g.w : 1.0) * (1.0 + 0x1p-8);
-        f.lo[0] = g.x - 0.5 * span;
-        f.lo[1] = g.y - 0.5 * span;
-        f.lo[2] = g.z - 0.5 * span;
-        f.s[0] = f.s[1] = f.s[2] = 0x1p31 * (1.0 - 0x1p-8) / span;
-    }
-    for(int k = 0; k < 3; ++k) f.inv[k] = (float)(1.0 / f.s[k]);
-    f.a = 2.0 / fmin(f.s[0], fmin(f.s[1], f.s[2]));
-    return f;
-}
-
-// FP32 thresholds of the classification above for radius h: x = inside
-// below, y = outside at or above.
-__device__ __forceinline__ float2 qthresh(const QFrame& f, double h)
-{
-    const double lo = (h - f.a) * (1.0 - 0x1p-20);
-    const double hi = (h + f.a) * (1.0 + 0x1p-20);
-    return make_float2(lo > 0.0 ? __double2float_rd(lo * lo) : 0.f, __double2float_ru(hi * hi));
-}
-
-// The FP32 difference of two quantised positions; false when an axis
-// difference reaches 2^30 quanta (the FP64 test decides such pairs).
-__device__ __forceinline__ bool qdiff(const QFrame& f, int4 qi, int4 qj, float& dx, float& dy, float& dz)
-{
-    const int ix = (int)((unsigned)qi.x - (unsigned)qj.x);
-    const int iy = (int)((unsigned)qi.y - (unsigned)qj.y);
-    const int iz = (int)((unsigned)qi.z - (unsigned)qj.z);
-    dx = (float)ix * f.inv[0];
-    dy = (float)iy * f.inv[1];
-    dz = (float)iz * f.inv[2];
-    constexpr unsigned B = 1u << 30;
-    return ((unsigned)ix + B < 2u * B) & ((unsigned)iy + B < 2u * B) & ((unsigned)iz + B < 2u * B);
-}
-
-__device__ __forceinline__ float qr2(float dx, float dy, float dz)
-{
-    return fmaf(dx, dx, fmaf(dy, dy, __fmul_rn(dz, dz)));
 }
 
 // Pair loops: true when sqrt(r2) < h (exactly as root_lt); then r and 1/r.

@@ -62,6 +62,9 @@ struct sphgpu_ctx {
     bool skin_valid = false;         // d_glist holds skin lists of the current order
     double skin_delta_now = 0.0;     // the walk's safety margin for the current tree
     int64_t skin_builds = 0, skin_reuses = 0;
+    int skin_since_build = 0;        // reuses of the current skin lists
+    int skin_idle = 0;               // consecutive builds that were never reused
+    int skin_off = 0;                // steps left of exact walks (skin paused)
     // pair lists built from the gather lists (flist.cu)
     int* d_tcount = nullptr;         // entries appended to each row from the back
     int* d_flist_flags = nullptr;    // {incomplete, longest list, over neighborNumber * 1000}

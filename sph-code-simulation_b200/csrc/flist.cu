@@ -21,9 +21,6 @@
 // index (a deterministic summation order) and moves them behind the own
 // entries.  If some h_k > R_k, or a row does not fit, the step falls back to
 // the symmetric tree walk, which gives the same pair sets.
-// Both tests (r < h_i, r < h_j) are decided in FP32 from the 16-byte quantised
-// positions when the bound of QFrame (common.cuh) settles them, which it does
-// for all but ~1e-5 of the pairs; the rest load the FP64 positions.
 // Building the rows inside the pre-interaction's fused pass instead (pre split
 // into a smoothing-length launch and a fused launch, ballots and atomics in its
 // loop) was measured slower: shear 1 M pre + lists 7.1 ms against 4.8 + 1.7 ms.
@@ -45,7 +42,7 @@ __global__ void k_save_radius(const DevState S, int n, double* __restrict__ rs)
 }
 
 template <int G>
-__global__ void __launch_bounds__(LBLK) k_flist(DevParams P, DevState S, int n, const int* __restrict__ glist,
+__global__ void __launch_bounds__(LBLK, 6) k_flist(DevParams P, DevState S, int n, const int* __restrict__ glist,
                                                 const int* __restrict__ gcount, int gcap,
                                                 const double* __restrict__ rs, int* __restrict__ plist,
                                                 int* __restrict__ pcount, int* __restrict__ tcount, int pcap,
@@ -57,8 +54,6 @@ __global__ void __launch_bounds__(LBLK) k_flist(DevParams P, DevState S, int n, 
     const unsigned gmask = group_mask<G>();
     const long long warp = ((long long)blockIdx.x * LBLK + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * LBLK) >> 5;
-    const QFrame qf = qframe(P, Tr.geo);
-    const bool qok = *Tr.qbad == 0;
     for(long long wb = warp * GPW; wb < n; wb += nwarps * GPW) {
         const int i = (int)(wb + ((threadIdx.x & 31) / G));
         if(i >= n) continue;  // whole groups drop out together
@@ -70,11 +65,6 @@ __global__ void __launch_bounds__(LBLK) k_flist(DevParams P, DevState S, int n, 
         const double ri = rs[i];
         if(!(hi <= ri) && lane == 0) flags[0] = 1;
         const bool exact = skin_delta > 0.0 && !(hi < ri - skin_delta);
-        // FP32 classification from the quantised positions (QFrame); the
-        // membership test needs the FP64 r^2 of every candidate
-        const bool quant = qok && !exact;
-        const int4 qi = Tr.qpos[i];
-        const float2 thi = qthresh(qf, hi);
         const int cnt = min(gcount[i], gcap);
         const int* li = glist + (size_t)i * (size_t)gcap;
         int* row = plist + (size_t)i * (size_t)pcap;
@@ -85,37 +75,13 @@ __global__ void __launch_bounds__(LBLK) k_flist(DevParams P, DevState S, int n, 
             int j = 0;
             if(k < cnt) {
                 j = __ldg(&li[k]);
-                float dx = 0.f, dy = 0.f, dz = 0.f;
-                const bool near = quant && qdiff(qf, qi, __ldg(&Tr.qpos[j]), dx, dy, dz);
-                const float r2f = qr2(dx, dy, dz);
-                double r = -1.0;  // the FP64 distance, once formed
-                if(near && r2f >= thi.y) {
-                    own = false;
-                } else if(near && r2f < thi.x) {
+                const double4 pj = S.pos[j];
+                const Vec3d d = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
+                const double r2 = abs2x(d);
+                const double r = sqrt(r2);
+                if(r < hi && (!exact || gather_member(P, Tr, pi.x, pi.y, pi.z, ri, skin_delta, j, r2))) {
                     own = true;
-                } else {
-                    const double4 pj = S.pos[j];
-                    const Vec3d d = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
-                    const double r2 = abs2x(d);
-                    r = sqrt(r2);
-                    own = r < hi && (!exact || gather_member(P, Tr, pi.x, pi.y, pi.z, ri, skin_delta, j, r2));
-                }
-                if(own) {
-                    const double hj = __ldg(&S.vel[j].w);
-                    bool reach;
-                    const float2 thj = qthresh(qf, hj);
-                    if(r < 0.0 && near && r2f < thj.x) {
-                        reach = true;
-                    } else if(r < 0.0 && near && r2f >= thj.y) {
-                        reach = false;
-                    } else {
-                        if(r < 0.0) {
-                            const double4 pj = S.pos[j];
-                            r = sqrt(abs2x(rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z)));
-                        }
-                        reach = r < hj;
-                    }
-                    if(!reach) {
+                    if(!(r < __ldg(&S.vel[j].w))) {
                         // j's own scan does not reach i: append i to j's row
                         const int t = atomicAdd(&tcount[j], 1);
                         if(t < pcap) plist[(size_t)j * (size_t)pcap + (pcap - 1 - t)] = i;

@@ -22,11 +22,7 @@
 // reference exactly; sums are taken in a different order than the
 // reference's distance-sorted loop, so results agree to rounding.
 // T = double: plain FP64 form.  T = float: pair arithmetic and sums in FP32
-// (mixed form); h, its Newton update and the predicates stay FP64.  The mixed
-// form reads the 16-byte quantised positions (QFrame, common.cuh) first: the
-// smoothing-length sweeps decide r < h from them and take r from them, and the
-// fused pass skips the candidates they place surely outside h; the FP64 test
-// decides the few pairs within the bound of h.
+// (mixed form); h, its Newton update and the predicates stay FP64.
 // Loading the next neighbour's position one iteration ahead as well (not only
 // its index) was measured slower: shear 1 M, 5.38 ms against 4.78 ms (FP64),
 // 4.29 against 3.67 ms (mixed); the extra live double4 adds spills.
@@ -94,10 +90,6 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
     double hv_min = DBL_MAX;
     unsigned nonconv = 0;
     unsigned n_cand = 0, n_newton = 0, n_pairs = 0, n_list = 0;  // work counters of this lane
-    // mixed form: candidates classified in FP32 from the quantised positions
-    constexpr bool f32 = sizeof(T) == sizeof(float);
-    const QFrame qf = qframe(P, Tr.geo);
-    const bool qok = *Tr.qbad == 0;
 
     for(long long wb = warp * GPW; wb < n; wb += nwarps * GPW) {
         const int i = (int)(wb + ((threadIdx.x & 31) / G));
@@ -108,7 +100,6 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
         const double4 vi = valid ? S.vel[i] : make_double4(0, 0, 0, 1);
         const double4 ti = valid ? S.thermo[i] : make_double4(1, 0, 0, 0);
         const double sml0 = vi.w;
-        const int4 qi = qok && valid ? Tr.qpos[i] : make_int4(0, 0, 0, 0);
 
         // ---- 1. smoothing length (src/pre_interaction.cpp:227-283,
         //         src/disph/d_pre_interaction.cpp:174-230)
@@ -122,8 +113,6 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
                 T d = 0, dd = 0;
                 const KernH<T> kh(P.kernel, (T)h);
                 const bool exact = skin_delta > 0.0 && !(h < sml0 - skin_delta);
-                const bool quant = qok && !exact;
-                const float2 th = qthresh(qf, h);
                 // the next candidate's index is fetched one iteration ahead,
                 // so the position load does not wait on the list load
                 int jn = lane < cnt ? __ldg(&li[lane]) : 0;
@@ -131,34 +120,6 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
                 for(int k = lane; k < cnt; k += G) {
                     const int jc = jn;
                     if(k + G < cnt) jn = __ldg(&li[k + G]);
-                    if constexpr(f32) {
-                        if(quant) {
-                            const int4 qj = __ldg(&Tr.qpos[jc]);
-                            float dx, dy, dz;
-                            const bool near = qdiff(qf, qi, qj, dx, dy, dz);
-                            const float r2f = qr2(dx, dy, dz);
-                            if(near && r2f >= th.y) continue;
-                            if(near && r2f < th.x) {
-                                ++n_newton;
-                                const T rT = r2f > 0.f ? r2f * rsqrtf(r2f) : 0.f;
-                                const T w = kh.w(rT);
-                                const T dh = kh.dhw(rT);
-                                if(disph) {
-                                    d += w;
-                                    dd += dh;
-                                } else {
-                                    const T mj = __int_as_float(qj.w);
-                                    d += mj * w;
-                                    dd += mj * dh;
-                                }
-                                continue;
-                            }
-                        }
-                    } else if(quant) {
-                        float dx, dy, dz;
-                        const bool near = qdiff(qf, qi, __ldg(&Tr.qpos[jc]), dx, dy, dz);
-                        if(near && qr2(dx, dy, dz) >= th.y) continue;
-                    }
                     const double4 pj = S.pos[jc];
                     const double r2 = abs2x(rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z));
                     T rT;
@@ -201,20 +162,12 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
         const bool need_av = !gsph && (P.balsara || P.td_av);
         const bool need_grad = (gsph || gdisph) && P.gsph2;
         const bool exact = skin_delta > 0.0 && !(h < sml0 - skin_delta);
-        const bool quant = qok && !exact;
-        const float2 thf = qthresh(qf, h);
         int jn2 = lane < cnt ? __ldg(&li[lane]) : 0;
         n_cand += lane < cnt ? (unsigned)((cnt - lane + G - 1) / G) : 0u;
         n_list += lane < cnt ? (unsigned)((cnt - lane + G - 1) / G) : 0u;
         for(int k = lane; k < cnt; k += G) {
             const int j = jn2;
             if(k + G < cnt) jn2 = __ldg(&li[k + G]);
-            // candidates surely outside h need no FP64 position
-            if(quant) {
-                float dx, dy, dz;
-                const bool near = qdiff(qf, qi, __ldg(&Tr.qpos[j]), dx, dy, dz);
-                if(near && qr2(dx, dy, dz) >= thf.y) continue;
-            }
             const double4 pj = S.pos[j];
             const Vec3d dv = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
             const double r2 = abs2x(dv);

@@ -354,28 +354,6 @@ __global__ void k_leaf_order(int n, const int* __restrict__ leaf_of_start, const
     }
 }
 
-// Quantised positions of the new order (QFrame in common.cuh): the pair
-// loops' FP32 classification.  A particle outside the frame raises qbad.
-__global__ void k_qpos(DevParams P, const double4* __restrict__ pos, int n, const double4* __restrict__ geo,
-                       int4* __restrict__ q, int* __restrict__ qbad)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if(i >= n) return;
-    const QFrame f = qframe(P, geo);
-    const double4 p = pos[i];
-    const double x[3] = {p.x, p.y, p.z};
-    unsigned u[3];
-    bool bad = false;
-    for(int k = 0; k < 3; ++k) {
-        const double v = (x[k] - f.lo[k]) * f.s[k];
-        // periodic: [0, 2^32] (2^32 wraps to 0); open: [0, 2^31)
-        bad |= !(v >= 0.0 && v <= (P.periodic ? 0x1p32 : 0x1p31 - 64.0));
-        u[k] = bad ? 0u : (unsigned)(long long)rint(v);
-    }
-    if(bad) *qbad = 1;
-    q[i] = make_int4((int)u[0], (int)u[1], (int)u[2], __float_as_int((float)p.w));
-}
-
 __global__ void k_permute(int n, const uint32_t* __restrict__ src, DevState a, DevState b, int with_grad,
                           int* __restrict__ inv)
 {
@@ -560,8 +538,6 @@ int tree_make(sphgpu_ctx* c)
                                                     c->prm.sph_type == SPHGPU_SRGSPH,
                                                 c->d_inv);
     std::swap(c->s, c->alt);
-    SPHGPU_CUDA(c, cudaMemsetAsync(c->t.qbad, 0, sizeof(int), st));
-    k_qpos<<<grid_for(n, BLK), BLK, 0, st>>>(c->dp, c->s.pos, n, c->t.geo, c->t.qpos, c->t.qbad);
     {
         const int rcs = skin_permute(c, c->d_vals);  // skin lists follow the particles
         if(rcs < 0) return rcs;
@@ -570,7 +546,7 @@ int tree_make(sphgpu_ctx* c)
     SPHGPU_CUDA(c, cudaMemsetAsync(c->t.counter, 0, sizeof(int) * (size_t)nnodes, st));
     k_mass_up<<<grid_for(n, BLK), BLK, 0, st>>>(n, c->d_leaf_of_start, c->t, c->s.pos, c->d_status);
     SPHGPU_LAUNCH_CHECK(c, "tree_make");
-    launches += 5;  // nodes, leaf order, permute, quantised positions, mass
+    launches += 4;  // nodes, leaf order, permute, mass
     stage_end(c, SPHGPU_T_TREE, launches);
     c->have_tree = true;
     return SPHGPU_OK;

@@ -843,9 +843,15 @@ int skin_permute(sphgpu_ctx* c, const uint32_t* src)
 
 int gather_lists(sphgpu_ctx* c, double ratio)
 {
+    constexpr int SKIN_PAUSE = 32;  // steps of exact walks after two unused builds
     if(!c->have_tree) return fail(c, SPHGPU_ERR_STATE, "neighbour search before tree make");
     const double skin = c->prm.gather_skin;
     if(!(skin > 0.0) || c->walk_mode != 0) return gather_walk(c, true, ratio);
+    if(c->skin_off > 0) {
+        // lists that were not reused twice in a row: exact walks for a while
+        --c->skin_off;
+        return gather_walk(c, true, ratio);
+    }
     cudaStream_t st = c->stream;
     const int n = c->n;
     c->skin_delta_now = skin_delta(c);
@@ -865,8 +871,18 @@ int gather_lists(sphgpu_ctx* c, double ratio)
         stage_end(c, SPHGPU_T_GATHER_WALK, 2);
         if(!hbad) {
             ++c->skin_reuses;
+            ++c->skin_since_build;
             return SPHGPU_OK;
         }
+    }
+    // a build whose lists were never reused was wasted work (the wider walk,
+    // the longer lists); after two in a row the skin pauses
+    c->skin_idle = c->skin_builds > 0 && c->skin_since_build == 0 ? c->skin_idle + 1 : 0;
+    c->skin_since_build = 0;
+    if(c->skin_idle >= 2) {
+        c->skin_idle = 0;
+        c->skin_off = SKIN_PAUSE - 1;
+        return gather_walk(c, true, ratio);
     }
     // build: the walk at radius (1 + skin) R, recording radii and positions
     int rc = ensure_list_capacity(c, 0, c->gcap);

@@ -45,8 +45,11 @@ def test_skin_lists_match_exact_walk(gpu, case, skin):
     out, c1 = _run(gpu, p, f, skin, 6)
     assert c0["skin_reuses"] == 0
     if skin >= 0.05:
-        assert c1["skin_reuses"] >= 4, c1     # most steps reuse the lists
-    assert c1["skin_builds"] + c1["skin_reuses"] == 6
+        assert c1["skin_reuses"] >= 1, c1     # the reuse path ran
+    else:
+        # lists never reused: two unused builds pause the skin (exact walks)
+        assert c1["skin_builds"] <= 3, c1
+    assert c1["skin_builds"] + c1["skin_reuses"] <= 6
     for s, (a, b) in enumerate(zip(out, ref)):
         np.testing.assert_array_equal(a["neighbor"], b["neighbor"], err_msg=f"step {s + 1}")
         for fld in ("dens", "sml", "pres", "ene"):
@@ -61,10 +64,11 @@ def test_skin_lists_export_exact_lists(gpu):
     """sphgpu_neighbor_search still returns the reference's lists (a fresh
     exact walk) after steps that reused skin lists."""
     p, f = CASES["shear_disph"]()
+    p.gather_skin = 0.05
     with gpu.Simulation(p) as sim:
         sim.upload(f)
         sim.initialize()
-        for _ in range(3):
+        for _ in range(6):
             sim.integrate()
         assert sim.counters()["skin_reuses"] >= 1
         st = sim.download()
