@@ -178,6 +178,9 @@ void free_all(sphgpu_ctx* c)
     c->skin_n = 0;
     c->skin_cap = 0;
     c->skin_valid = false;
+    c->skin_map_pending = false;
+    c->skin_built = false;
+    c->skin_since_build = c->skin_idle = c->skin_off = 0;
 }
 
 template <typename T>
@@ -574,12 +577,15 @@ int sphgpu_upload(sphgpu_ctx* c, int64_t n, const double* const* fields)
     }
     k_put_all<<<grid_for(n, 256), 256, 0, c->stream>>>(c->s, F, (int)n);
     SPHGPU_LAUNCH_CHECK(c, "upload");
+    // skin lists stay valid across an upload of the same particle count:
+    // their rows follow the particles into caller order at the next tree
+    // build, and the displacement check against their build positions holds
+    // whatever the uploaded positions are
+    if((rc = skin_upload(c)) < 0) return rc;
     SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
     c->have_tree = false;
     c->flist_ready = false;
     c->first_pre = true;
-    c->skin_valid = false;
-    c->skin_since_build = c->skin_idle = c->skin_off = 0;
     c->time = 0.0;
     return SPHGPU_OK;
 }

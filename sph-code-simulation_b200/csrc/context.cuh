@@ -62,6 +62,10 @@ struct sphgpu_ctx {
     bool skin_valid = false;         // d_glist holds skin lists of the current order
     double skin_delta_now = 0.0;     // the walk's safety margin for the current tree
     int64_t skin_builds = 0, skin_reuses = 0;
+    uint32_t* d_skin_map = nullptr;  // after an upload: caller index -> list row
+    uint32_t* d_skin_src = nullptr;  // composed permutation (scratch)
+    bool skin_map_pending = false;   // d_skin_map applies at the next permutation
+    bool skin_built = false;         // a skin build happened since the buffers were made
     int skin_since_build = 0;        // reuses of the current skin lists
     int skin_idle = 0;               // consecutive builds that were never reused
     int skin_off = 0;                // steps left of exact walks (skin paused)
@@ -205,6 +209,7 @@ int gather_lists(sphgpu_ctx* c, double ratio);
 // Move valid skin lists to the order of a new tree (src: old position of the
 // particle now at each position).
 int skin_permute(sphgpu_ctx* c, const uint32_t* src);
+int skin_upload(sphgpu_ctx* c);
 int pair_walk(sphgpu_ctx* c);
 int export_lists(sphgpu_ctx* c, int which, int64_t* offsets, int32_t* ids, int64_t cap);
 int exhaustive_lists(sphgpu_ctx* c, int is_ij, int64_t* offsets, int32_t* ids, int64_t cap);

@@ -28,7 +28,12 @@
 // the second pass over the nodes costs more than the divergence it removes);
 // lanes that park on an opened leaf until 5 / 10 / 16 lanes are parked and
 // then compute their next pairs together (169 / 225 / 286 ms: parked lanes
-// idle far longer than the divergent pairs take).
+// idle far longer than the divergent pairs take).  Kept: the squared edge of
+// each level from a table in shared memory instead of an ldexp per node, and
+// the next node's records loaded as soon as the opening test has chosen it
+// (116.0 -> 114.9 ms together; capped at 6 resident blocks the prefetching
+// walk spills and takes 124.8 ms).  The walk waits on its FP64 dependency
+// chains (the correctly rounded square roots and divisions), not on loads.
 #include <cuda_runtime.h>
 
 #include "context.cuh"
@@ -62,51 +67,71 @@ __global__ void __launch_bounds__(GBLK) k_gravity(DevParams P, DevState S, DevTr
     double ax = acc.x, ay = acc.y, az = acc.z, phi = 0.0;
     const double G = P.G;
     const int nnodes = *Tr.nnodes;
-    // node edges halve exactly per level: edge(L) = root edge * 2^(1 - L)
-    const double root_edge = ldg4(&Tr.geo[0]).w;
+    // node edges halve exactly per level: edge(L) = root edge * 2^(1 - L);
+    // the squared edge of every level, as the opening test forms it
+    __shared__ double s_l2[256];
+    {
+        const double root_edge = ldg4(&Tr.geo[0]).w;
+        for(int L = threadIdx.x; L < 256; L += GBLK) {
+            const double e = ldexp(root_edge, 1 - L);
+            s_l2[L] = e * e;
+        }
+        __syncthreads();
+    }
     int nd = valid ? 0 : nnodes, steps = 0;
     unsigned n_mono = 0, n_leaf = 0;  // work counters of this lane (steps = nodes met)
+    // the records of the node in hand; the next node's are loaded as soon as
+    // the opening test has chosen it, before this node's terms are formed
+    int4 lk = make_int4(0, 0, nnodes, 0);
+    double4 mc = make_double4(0, 0, 0, 0);
+    if(nd < nnodes) {
+        lk = __ldg(&Tr.link[nd]);
+        mc = ldg4(&Tr.mass[nd]);
+    }
     while(nd < nnodes) {
         if(++steps > nnodes) {  // corrupt node table: report, never loop
             atomicOr(&st->pass_guard, PASS_GUARD_GRAVITY);
             break;
         }
-        const int4 lk = __ldg(&Tr.link[nd]);
         const bool leaf = (lk.w >> 8) != 0;
-        bool open = false;
-        {
-            const double edge = ldexp(root_edge, 1 - (lk.w & 0xff));
-            const double4 mc = ldg4(&Tr.mass[nd]);
-            const Vec3d d = rij(P, xi, yi, zi, mc.x, mc.y, mc.z);
-            const double l2 = edge * edge;
-            const double d2 = d.x * d.x + d.y * d.y + d.z * d.z;
-            open = (l2 > P.theta2 * d2) || (d2 < l2);
-            if(!open) {
-                ++n_mono;
-                const double rinv = 1.0 / sqrt(d2);
-                phi -= G * mc.w * rinv;
-                const double s = G * mc.w * (rinv * rinv * rinv);
-                ax -= d.x * s;
-                ay -= d.y * s;
-                az -= d.z * s;
-            }
-            if(open && leaf) {
-                n_leaf += (unsigned)(lk.y - lk.x) - ((i >= lk.x && i < lk.y) ? 1u : 0u);
-                for(int q = lk.x; q < lk.y; ++q) {
-                    if(q == i) continue;
-                    const double4 pq = ldg4(&S.pos[q]);
-                    const double hq = ldg4(&S.vel[q]).w;
-                    const Vec3d r = rij(P, xi, yi, zi, pq.x, pq.y, pq.z);
-                    const double rr = sqrt(r.x * r.x + r.y * r.y + r.z * r.z);
-                    phi -= G * pq.w * (hk_f<double>(rr, hi) + hk_f<double>(rr, hq)) * 0.5;
-                    const double c = G * pq.w * (hk_g<double>(rr, hi) + hk_g<double>(rr, hq)) * 0.5;
-                    ax -= r.x * c;
-                    ay -= r.y * c;
-                    az -= r.z * c;
-                }
+        const Vec3d d = rij(P, xi, yi, zi, mc.x, mc.y, mc.z);
+        const double l2 = s_l2[lk.w & 0xff];
+        const double d2 = d.x * d.x + d.y * d.y + d.z * d.z;
+        const bool open = (l2 > P.theta2 * d2) || (d2 < l2);
+        const int next = (open && !leaf) ? nd + 1 : lk.z;
+        int4 lk_n = lk;
+        double4 mc_n = mc;
+        if(next < nnodes) {
+            lk_n = __ldg(&Tr.link[next]);
+            mc_n = ldg4(&Tr.mass[next]);
+        }
+        if(!open) {
+            ++n_mono;
+            const double rinv = 1.0 / sqrt(d2);
+            phi -= G * mc.w * rinv;
+            const double s = G * mc.w * (rinv * rinv * rinv);
+            ax -= d.x * s;
+            ay -= d.y * s;
+            az -= d.z * s;
+        }
+        if(open && leaf) {
+            n_leaf += (unsigned)(lk.y - lk.x) - ((i >= lk.x && i < lk.y) ? 1u : 0u);
+            for(int q = lk.x; q < lk.y; ++q) {
+                if(q == i) continue;
+                const double4 pq = ldg4(&S.pos[q]);
+                const double hq = __ldg(&S.vel[q].w);
+                const Vec3d r = rij(P, xi, yi, zi, pq.x, pq.y, pq.z);
+                const double rr = sqrt(r.x * r.x + r.y * r.y + r.z * r.z);
+                phi -= G * pq.w * (hk_f<double>(rr, hi) + hk_f<double>(rr, hq)) * 0.5;
+                const double c = G * pq.w * (hk_g<double>(rr, hi) + hk_g<double>(rr, hq)) * 0.5;
+                ax -= r.x * c;
+                ay -= r.y * c;
+                az -= r.z * c;
             }
         }
-        nd = (open && !leaf) ? nd + 1 : lk.z;
+        nd = next;
+        lk = lk_n;
+        mc = mc_n;
     }
     if(valid) {
         S.acc[i] = make_double4(ax, ay, az, acc.w);

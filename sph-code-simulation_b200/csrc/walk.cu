@@ -721,6 +721,13 @@ __global__ void k_skin_check(DevParams P, DevState S, int n, const double* __res
 
 // Lists, counts, radii and build positions of the previous particle order
 // moved to the order of the new tree (particle q now at p = new_of_old[q]).
+__global__ void k_skin_compose(const uint32_t* __restrict__ src, const uint32_t* __restrict__ map, int n,
+                               uint32_t* __restrict__ out)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p < n) out[p] = map[src[p]];
+}
+
 __global__ void k_skin_new_of_old(const uint32_t* __restrict__ src, int n, int* __restrict__ new_of_old)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -742,18 +749,29 @@ __global__ void k_skin_permute(const uint32_t* __restrict__ src, int n, int cap,
     const int* a = list + (size_t)q * (size_t)cap;
     int* b = list2 + (size_t)p * (size_t)cap;
     if((cap & 3) == 0) {
-        // rows start on 16 bytes: four entries per lane and load, four
-        // independent gathers in flight (entries past cnt are copied as is)
+        // rows start on 16 bytes: two 16-byte loads of four entries per lane,
+        // then eight independent gathers in flight (entries past cnt are
+        // copied as is)
         const int4* a4 = reinterpret_cast<const int4*>(a);
         int4* b4 = reinterpret_cast<int4*>(b);
-        for(int e = lane; 4 * e < cnt; e += 32) {
+        for(int e = lane; 4 * e < cnt; e += 64) {
+            const int e2 = e + 32;
+            const bool two = 4 * e2 < cnt;
             int4 v = __ldg(&a4[e]);
-            const int k = 4 * e;
+            int4 u = two ? __ldg(&a4[e2]) : make_int4(0, 0, 0, 0);
+            const int k = 4 * e, k2 = 4 * e2;
             v.x = __ldg(&new_of_old[v.x]);
             if(k + 1 < cnt) v.y = __ldg(&new_of_old[v.y]);
             if(k + 2 < cnt) v.z = __ldg(&new_of_old[v.z]);
             if(k + 3 < cnt) v.w = __ldg(&new_of_old[v.w]);
+            if(two) {
+                u.x = __ldg(&new_of_old[u.x]);
+                if(k2 + 1 < cnt) u.y = __ldg(&new_of_old[u.y]);
+                if(k2 + 2 < cnt) u.z = __ldg(&new_of_old[u.z]);
+                if(k2 + 3 < cnt) u.w = __ldg(&new_of_old[u.w]);
+            }
             b4[e] = v;
+            if(two) b4[e2] = u;
         }
     } else {
         for(int e = lane; e < cnt; e += 32) b[e] = __ldg(&new_of_old[__ldg(&a[e])]);
@@ -780,41 +798,49 @@ double skin_delta(sphgpu_ctx* c)
 
 int skin_alloc(sphgpu_ctx* c)
 {
-    const int64_t want = (int64_t)c->n * c->gcap;
-    if(c->skin_n == c->n && c->skin_cap == c->gcap && c->d_skin) return SPHGPU_OK;
-    if(c->d_skin) {
-        SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
-        SPHGPU_CUDA(c, cudaFree(c->d_skin));
-        c->d_skin = nullptr;
-    }
-    if(c->d_glist_alt) {
-        SPHGPU_CUDA(c, cudaFree(c->d_glist_alt));
-        c->d_glist_alt = nullptr;
-    }
-    // the second list buffer is an allocation of its own: it trades places
-    // with d_glist at every permutation
-    SPHGPU_CUDA(c, cudaMalloc(&c->d_glist_alt, std::max<size_t>(4 * (size_t)want, 4)));
+    // per-particle arrays (build radius and position, counts, permutation
+    // scratch) follow n; the second list buffer follows n x capacity, and is
+    // an allocation of its own: it trades places with d_glist at every
+    // permutation
     const size_t n = (size_t)c->n;
-    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
-    const size_t bytes = al(4 * n) + 2 * al(8 * n) + 2 * al(32 * n) + al(4 * n) + 256;
-    SPHGPU_CUDA(c, cudaMalloc(&c->d_skin, bytes));
-    char* b = static_cast<char*>(c->d_skin);
-    size_t off = 0;
-    auto take = [&](size_t sz) {
-        char* q = b + off;
-        off += al(sz);
-        return q;
-    };
-    c->d_gcount_alt = reinterpret_cast<int*>(take(4 * n));
-    c->d_skin_r = reinterpret_cast<double*>(take(8 * n));
-    c->d_skin_r_alt = reinterpret_cast<double*>(take(8 * n));
-    c->d_skin_x = reinterpret_cast<double4*>(take(32 * n));
-    c->d_skin_x_alt = reinterpret_cast<double4*>(take(32 * n));
-    c->d_skin_new = reinterpret_cast<int*>(take(4 * n));
-    c->d_skin_scal = reinterpret_cast<double*>(take(16));
-    c->skin_n = c->n;
-    c->skin_cap = c->gcap;
-    c->skin_valid = false;
+    if(c->skin_n != c->n || !c->d_skin) {
+        if(c->d_skin) {
+            SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+            SPHGPU_CUDA(c, cudaFree(c->d_skin));
+            c->d_skin = nullptr;
+        }
+        auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+        const size_t bytes = al(4 * n) + 2 * al(8 * n) + 2 * al(32 * n) + 3 * al(4 * n) + 256;
+        SPHGPU_CUDA(c, cudaMalloc(&c->d_skin, bytes));
+        char* b = static_cast<char*>(c->d_skin);
+        size_t off = 0;
+        auto take = [&](size_t sz) {
+            char* q = b + off;
+            off += al(sz);
+            return q;
+        };
+        c->d_gcount_alt = reinterpret_cast<int*>(take(4 * n));
+        c->d_skin_r = reinterpret_cast<double*>(take(8 * n));
+        c->d_skin_r_alt = reinterpret_cast<double*>(take(8 * n));
+        c->d_skin_x = reinterpret_cast<double4*>(take(32 * n));
+        c->d_skin_x_alt = reinterpret_cast<double4*>(take(32 * n));
+        c->d_skin_new = reinterpret_cast<int*>(take(4 * n));
+        c->d_skin_map = reinterpret_cast<uint32_t*>(take(4 * n));
+        c->d_skin_src = reinterpret_cast<uint32_t*>(take(4 * n));
+        c->d_skin_scal = reinterpret_cast<double*>(take(16));
+        c->skin_n = c->n;
+        c->skin_valid = false;
+        c->skin_map_pending = false;
+    }
+    if(c->skin_cap != c->gcap || !c->d_glist_alt) {
+        if(c->d_glist_alt) {
+            SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
+            SPHGPU_CUDA(c, cudaFree(c->d_glist_alt));
+            c->d_glist_alt = nullptr;
+        }
+        SPHGPU_CUDA(c, cudaMalloc(&c->d_glist_alt, std::max<size_t>(4 * n * (size_t)c->gcap, 4)));
+        c->skin_cap = c->gcap;
+    }
     return SPHGPU_OK;
 }
 
@@ -826,6 +852,13 @@ int skin_permute(sphgpu_ctx* c, const uint32_t* src)
         return SPHGPU_OK;
     }
     const int n = c->n;
+    if(c->skin_map_pending) {
+        // an upload put the particles in caller order since the lists were
+        // last moved: compose that step with this one
+        k_skin_compose<<<grid_for(n, 256), 256, 0, c->stream>>>(src, c->d_skin_map, n, c->d_skin_src);
+        src = c->d_skin_src;
+        c->skin_map_pending = false;
+    }
     k_skin_new_of_old<<<grid_for(n, 256), 256, 0, c->stream>>>(src, n, c->d_skin_new);
     k_skin_permute<<<grid_for((long long)n * 32, 256), 256, 0, c->stream>>>(
         src, n, (int)c->gcap, c->d_skin_new, c->d_glist, c->d_gcount, c->d_skin_r, c->d_skin_x, c->d_glist_alt,
@@ -838,6 +871,18 @@ int skin_permute(sphgpu_ctx* c, const uint32_t* src)
     std::swap(c->d_skin_x, c->d_skin_x_alt);
     c->stage_launch[SPHGPU_T_TREE] += 2;
     c->launches += 2;
+    return SPHGPU_OK;
+}
+
+int skin_upload(sphgpu_ctx* c)
+{
+    // the lists keep their rows; the row of the particle now at caller index
+    // k is its octree position before the upload (inv), applied at the next
+    // tree build together with that build's own permutation
+    if(!c->skin_valid || c->skin_map_pending) return SPHGPU_OK;
+    SPHGPU_CUDA(c, cudaMemcpyAsync(c->d_skin_map, c->d_inv, sizeof(int) * (size_t)c->n, cudaMemcpyDeviceToDevice,
+                                   c->stream));
+    c->skin_map_pending = true;
     return SPHGPU_OK;
 }
 
@@ -877,7 +922,7 @@ int gather_lists(sphgpu_ctx* c, double ratio)
     }
     // a build whose lists were never reused was wasted work (the wider walk,
     // the longer lists); after two in a row the skin pauses
-    c->skin_idle = c->skin_builds > 0 && c->skin_since_build == 0 ? c->skin_idle + 1 : 0;
+    c->skin_idle = c->skin_built && c->skin_since_build == 0 ? c->skin_idle + 1 : 0;
     c->skin_since_build = 0;
     if(c->skin_idle >= 2) {
         c->skin_idle = 0;
@@ -896,13 +941,12 @@ int gather_lists(sphgpu_ctx* c, double ratio)
     stage_end(c, SPHGPU_T_GATHER_WALK, launches);
     if(rc == SPHGPU_ERR_NEIGHBOR_OVERFLOW) return gather_walk(c, true, ratio);  // decided on the exact lists
     if(rc < 0) return rc;
-    if(c->skin_n != c->n || c->skin_cap != c->gcap) {
-        // the walk grew the lists past the skin buffers: take exact lists for
-        // this step (consumers treat lists as skin lists only while
-        // skin_valid); the buffers follow at the next build
-        return gather_walk(c, true, ratio);
-    }
+    // the walk may have grown the list capacity: the second list buffer
+    // follows (the recorded radii and positions are per particle and stand)
+    const int ra = skin_alloc(c);
+    if(ra < 0) return ra;
     c->skin_valid = true;
+    c->skin_built = true;
     ++c->skin_builds;
     return rc;
 }

@@ -83,3 +83,44 @@ def test_skin_lists_export_exact_lists(gpu):
     n = len(off) - 1
     rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(off))
     np.testing.assert_array_equal(np.sort(rows * n + ids), np.sort(rows * n + ids2))
+
+
+def test_skin_lists_survive_uploads(gpu):
+    """An upload of the same particle count keeps the skin lists (their rows
+    follow the particles into caller order at the next tree build); an
+    upload that moves particles past the skin forces a rebuild.  Steps with
+    an upload before each equal those with exact walks."""
+    p, f = CASES["evrard_disph"]()
+    runs = []
+    for skin in (0.0, 0.05):
+        q = p.copy()
+        q.gather_skin = skin
+        with gpu.Simulation(q) as sim:
+            sim.upload(f)
+            sim.initialize()
+            sim.reset_counters()
+            outs = []
+            moved = None
+            for s in range(6):
+                st = {k: v for k, v in sim.download().items() if not k.startswith("sr_")}
+                if s == 3:
+                    # a few particles moved by about one smoothing length
+                    st["pos_x"] = st["pos_x"].copy()
+                    st["pos_x"][:40] += 0.1
+                    before = sim.counters()["skin_builds"]
+                sim.upload(st)
+                sim.set_initial_smoothing(False)
+                sim.integrate()
+                if s == 3:
+                    moved = sim.counters()["skin_builds"] - before
+                outs.append(sim.download())
+            runs.append((outs, sim.counters(), moved))
+    (ref, c0, _), (out, c1, moved) = runs
+    assert c0["skin_reuses"] == 0
+    # initialize built the lists; the steps around the move reuse them
+    assert c1["skin_reuses"] >= 3, c1
+    assert moved == 1, moved   # the moved particles outran the skin: one rebuild
+    for s, (a, b) in enumerate(zip(out, ref)):
+        np.testing.assert_array_equal(a["neighbor"], b["neighbor"], err_msg=f"step {s + 1}")
+        for fld in ("dens", "sml", "pres", "ene"):
+            _close(a[fld], b[fld], f"step {s + 1} {fld}", median=1e-12, p999=1e-9, worst=1e-6)
