@@ -208,11 +208,14 @@ __device__ void riemann_iterative(const double* L, const double* R, double gamma
 // learned guess, deferring the pairs whose linearised start the screen
 // rejects (their features and pair slots go to the MlpPairs rows); 4 = the
 // deferred pairs only, with the network's guess, added to acc.
-// Minimum resident blocks per SM (caps registers; measured on B200).
+// Minimum resident blocks per SM (caps registers; measured on B200).  The
+// FP64 disph force takes 2 (27.2 -> 24.5 ms on the 8.78 M sphere, no slower on
+// the 1 M shear layer); its FP32 form stays at 4 (3: 17.2 -> 17.5 ms).
 template <typename T, int TYPE>
 constexpr int force_min_blocks()
 {
-    return (sizeof(T) == sizeof(float) || TYPE == SPHGPU_GSPH || TYPE == SPHGPU_GDISPH) ? 4 : 3;
+    if(sizeof(T) == sizeof(float) || TYPE == SPHGPU_GSPH || TYPE == SPHGPU_GDISPH) return 4;
+    return TYPE == SPHGPU_DISPH ? 2 : 3;
 }
 
 // The particles a launch computes: all n, or (sub.idx != null) the listed

@@ -61,10 +61,14 @@ __device__ __forceinline__ bool sweep_r(double r2, double h, float& r)
     return true;
 }
 
-// Minimum resident blocks per SM (caps registers; measured on B200).
+// Minimum resident blocks per SM (caps registers; measured on B200).  disph
+// takes fewer, wider blocks than the rest: on the 8.78 M sphere FP64 2 blocks
+// (no spills) against 3 took 34.6 against 40.3 ms, FP32 3 against 4 28.7
+// against 30.6 ms; the 1 M shear layer was no slower.
 template <typename T, int TYPE>
 constexpr int pre_min_blocks()
 {
+    if(TYPE == SPHGPU_DISPH) return sizeof(T) == sizeof(float) ? 3 : 2;
     return (sizeof(T) == sizeof(float) && TYPE != SPHGPU_GSPH && TYPE != SPHGPU_GDISPH) ? 4 : 3;
 }
 
