@@ -138,12 +138,15 @@ constexpr int PASS_GUARD_KSIZE = 2;      // bottom-up kernel_size (set_kernel)
 constexpr int PASS_GUARD_GRAVITY = 4;    // Barnes-Hut walk (FP64)
 constexpr int PASS_GUARD_GRAVITY32 = 8;  // Barnes-Hut walk (mixed form)
 
-// Read-only 32-byte load through the non-coherent path (two 16-byte halves).
+// Read-only 32-byte load through the non-coherent path, one 256-bit access
+// (sm_100).  p must be 32-byte aligned: every double4 array here is an
+// allocation of its own (256-byte aligned) indexed by element.  Only for data
+// that no thread of the kernel writes, or whose read components it does not.
 __device__ __forceinline__ double4 ldg4(const double4* p)
 {
-    const double2* q = reinterpret_cast<const double2*>(p);
-    const double2 a = __ldg(q), b = __ldg(q + 1);
-    return make_double4(a.x, a.y, b.x, b.y);
+    double4 r;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w) : "l"(p));
+    return r;
 }
 
 // ------------------------------------------------------------ exact FP64

@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(LBLK, 6) k_flist(DevParams P, DevState S, int 
             int j = 0;
             if(k < cnt) {
                 j = __ldg(&li[k]);
-                const double4 pj = S.pos[j];
+                const double4 pj = ldg4(&S.pos[j]);
                 const Vec3d d = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
                 const double r2 = abs2x(d);
                 const double r = sqrt(r2);

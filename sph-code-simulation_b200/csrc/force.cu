@@ -208,13 +208,14 @@ __device__ void riemann_iterative(const double* L, const double* R, double gamma
 // learned guess, deferring the pairs whose linearised start the screen
 // rejects (their features and pair slots go to the MlpPairs rows); 4 = the
 // deferred pairs only, with the network's guess, added to acc.
-// Minimum resident blocks per SM (caps registers; measured on B200).  The
-// FP64 disph force takes 2 (27.2 -> 24.5 ms on the 8.78 M sphere, no slower on
-// the 1 M shear layer); its FP32 form stays at 4 (3: 17.2 -> 17.5 ms).
+// Minimum resident blocks per SM (caps registers; measured on B200): FP64
+// disph 2 (27.2 -> 24.5 ms on the 8.78 M sphere), FP64 gdisph 3 (8.8 -> 7.7 ms
+// on the 2 M tube), gsph and the FP32 forms 4 (gsph 18.8 -> 9.6 ms against 3;
+// FP32 disph 17.2 against 17.5 ms with 3), FP64 ssph 3.
 template <typename T, int TYPE>
 constexpr int force_min_blocks()
 {
-    if(sizeof(T) == sizeof(float) || TYPE == SPHGPU_GSPH || TYPE == SPHGPU_GDISPH) return 4;
+    if(sizeof(T) == sizeof(float) || TYPE == SPHGPU_GSPH) return 4;
     return TYPE == SPHGPU_DISPH ? 2 : 3;
 }
 
@@ -284,9 +285,9 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
                 yq = mp.y[mp.svals[row]];
             }
             const int j = li[kk];
-            const double4 pj = S.pos[j];
+            const double4 pj = ldg4(&S.pos[j]);
             const Vec3d d = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
-            const double4 vj = S.vel[j];
+            const double4 vj = ldg4(&S.vel[j]);
             const double hj = vj.w;
             double r, rinv;
             if constexpr(f32) {
@@ -304,7 +305,7 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
                 rinv = 1.0 / r;
             }
             ++n_pairs;
-            const double4 tj = S.thermo[j];
+            const double4 tj = ldg4(&S.thermo[j]);
             const T rT = (T)r;
             const T rinvT = (T)rinv;
             const V3<T> rv{(T)d.x, (T)d.y, (T)d.z};
@@ -326,8 +327,8 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
                 double Lst[4], Rst[4];
                 if(P.gsph2) {
                     // MUSCL reconstruction (src/gsph/g_fluid_force.cpp:103-140)
-                    const double4 gj0 = S.grad[j], gj1 = S.grad[(size_t)n + j];
-                    const double4 gj2 = S.grad[2 * (size_t)n + j], gj3 = S.grad[3 * (size_t)n + j];
+                    const double4 gj0 = ldg4(&S.grad[j]), gj1 = ldg4(&S.grad[(size_t)n + j]);
+                    const double4 gj2 = ldg4(&S.grad[2 * (size_t)n + j]), gj3 = ldg4(&S.grad[3 * (size_t)n + j]);
                     const T di = T(0.5) * (T(1) - ci * (T)dt * (T)rinv);
                     const T dj = T(0.5) * (T(1) - cj * (T)dt * (T)rinv);
                     const T exT = (T)ex, eyT = (T)ey, ezT = (T)ez;
@@ -455,7 +456,7 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
                     continue;
                 }
             }
-            const double4 sj = S.visc[j];
+            const double4 sj = ldg4(&S.visc[j]);
             const V3<T> dwij{(dwi.x + dwj.x) * T(0.5), (dwi.y + dwj.y) * T(0.5), (dwi.z + dwj.z) * T(0.5)};
             const V3<T> vij{(T)(vi.x - vj.x), (T)(vi.y - vj.y), (T)(vi.z - vj.z)};
             // artificial viscosity (src/fluid_force.cpp:88-106)

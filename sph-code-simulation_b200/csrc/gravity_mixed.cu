@@ -141,8 +141,12 @@ __global__ void __launch_bounds__(MBLK, 8) k_gravity_mixed(DevParams P, DevState
             atomicOr(&st->pass_guard, PASS_GUARD_GRAVITY32);
             break;
         }
-        const float4 a = __ldg(&rec[nd].a);
-        const int4 b = __ldg(&rec[nd].b);
+        float4 a;
+        int4 b;
+        // the 32-byte record in one 256-bit access
+        asm("ld.global.nc.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+            : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+            : "l"(rec + nd));
         const bool leaf = (b.y >> 16) & 1;
         const float l2 = __int_as_float(b.w);
         float dx = (xh - a.x) + (xl - __uint_as_float((unsigned)b.x << 16));

@@ -61,15 +61,16 @@ __device__ __forceinline__ bool sweep_r(double r2, double h, float& r)
     return true;
 }
 
-// Minimum resident blocks per SM (caps registers; measured on B200).  disph
-// takes fewer, wider blocks than the rest: on the 8.78 M sphere FP64 2 blocks
-// (no spills) against 3 took 34.6 against 40.3 ms, FP32 3 against 4 28.7
-// against 30.6 ms; the 1 M shear layer was no slower.
+// Minimum resident blocks per SM (caps registers; measured on B200).  The
+// FP64 forms of disph, gsph and gdisph take 2 (no spills): 8.78 M sphere
+// disph 40.3 -> 34.6 ms, 2 M tubes gsph 4.5 -> 3.7, gdisph 6.7 -> 4.3 ms; the
+// 1 M shear layer no slower.  FP32: disph 3 (30.6 -> 28.7 ms), gsph / gdisph 3
+// (2 is slower), ssph 4.
 template <typename T, int TYPE>
 constexpr int pre_min_blocks()
 {
-    if(TYPE == SPHGPU_DISPH) return sizeof(T) == sizeof(float) ? 3 : 2;
-    return (sizeof(T) == sizeof(float) && TYPE != SPHGPU_GSPH && TYPE != SPHGPU_GDISPH) ? 4 : 3;
+    if(sizeof(T) == sizeof(double)) return TYPE == SPHGPU_SSPH ? 3 : 2;
+    return TYPE == SPHGPU_SSPH ? 4 : 3;
 }
 
 // skin_delta > 0: the lists are skin lists (supersets of the gather lists);
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
                 for(int k = lane; k < cnt; k += G) {
                     const int jc = jn;
                     if(k + G < cnt) jn = __ldg(&li[k + G]);
-                    const double4 pj = S.pos[jc];
+                    const double4 pj = ldg4(&S.pos[jc]);
                     const double r2 = abs2x(rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z));
                     T rT;
                     if(sweep_r(r2, h, rT) && (!exact || gather_member(P, Tr, pi.x, pi.y, pi.z, sml0, skin_delta, jc, r2))) {
@@ -172,7 +173,7 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
         for(int k = lane; k < cnt; k += G) {
             const int j = jn2;
             if(k + G < cnt) jn2 = __ldg(&li[k + G]);
-            const double4 pj = S.pos[j];
+            const double4 pj = ldg4(&S.pos[j]);
             const Vec3d dv = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
             const double r2 = abs2x(dv);
             double r, rinv;
@@ -188,8 +189,9 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
             }
             if(exact && !gather_member(P, Tr, pi.x, pi.y, pi.z, sml0, skin_delta, j, r2)) continue;
             ++nn;
-            const double4 vj = S.vel[j];
-            const double4 tj = S.thermo[j];
+            // neighbours' velocities and u, c_s: components no thread here writes
+            const double4 vj = ldg4(&S.vel[j]);
+            const double4 tj = ldg4(&S.thermo[j]);
             const T rT = (T)r;
             const T w = kh.w(rT);
             const T mj = (T)pj.w;
