@@ -286,6 +286,17 @@ int sphgpu_initialize(sphgpu_ctx* ctx);
 /* Solver::integrate (src/solver.cpp:966-978) followed by
    Simulation::update_time. */
 int sphgpu_integrate(sphgpu_ctx* ctx);
+/* One sphgpu_integrate on host buffers, for a host that keeps the particle
+   state (the reference's Solver::integrate with every module on the GPU and
+   SPHParticle as the record): in_fields replace the device state as
+   sphgpu_upload does, except that the simulation time and the
+   initial-smoothing flag carry on (the particle count must be the uploaded
+   one); the step runs; out_fields receive the state as sphgpu_download
+   writes it.  Fields that are final early in the step (positions and mass
+   after the tree build, the PreInteraction outputs after it) are copied to
+   the host while the rest of the step runs, on a second stream; the call
+   returns when every copy is done.  Either table may hold NULL entries. */
+int sphgpu_integrate_host(sphgpu_ctx* ctx, const double* const* in_fields, double* const* out_fields);
 /* Solver::compute_total_energies (src/solver.cpp:1149-1175), plus total
    momentum (mom[3]); FP64 device reductions. mom may be NULL. */
 int sphgpu_energies(sphgpu_ctx* ctx, double* kinetic, double* thermal,

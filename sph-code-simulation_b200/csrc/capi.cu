@@ -332,36 +332,47 @@ __global__ void k_get_all(DevState S, FieldSlots F, int n)
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= n) return;
     const int dst = S.id[i];
-    auto put4 = [&](int f0, double4 v) {
-        if(F.p[f0]) F.p[f0][dst] = v.x;
-        if(F.p[f0 + 1]) F.p[f0 + 1][dst] = v.y;
-        if(F.p[f0 + 2]) F.p[f0 + 2][dst] = v.z;
-    };
     auto put1 = [&](int f, double v) {
         if(F.p[f]) F.p[f][dst] = v;
     };
-    const double4 pos = S.pos[i], vel = S.vel[i], acc = S.acc[i], velp = S.velp[i], th = S.thermo[i],
-                  vs = S.visc[i];
-    put4(SPHGPU_F_POS_X, pos);
-    put1(SPHGPU_F_MASS, pos.w);
-    put4(SPHGPU_F_VEL_X, vel);
-    put1(SPHGPU_F_SML, vel.w);
-    put4(SPHGPU_F_ACC_X, acc);
-    put1(SPHGPU_F_DENE, acc.w);
-    put4(SPHGPU_F_VELP_X, velp);
-    put1(SPHGPU_F_ENE_P, velp.w);
-    put1(SPHGPU_F_DENS, th.x);
-    put1(SPHGPU_F_PRES, th.y);
-    put1(SPHGPU_F_ENE, th.z);
-    put1(SPHGPU_F_SOUND, th.w);
-    put1(SPHGPU_F_ALPHA, vs.x);
-    put1(SPHGPU_F_BALSARA, vs.y);
-    put1(SPHGPU_F_GRADH, vs.z);
-    put1(SPHGPU_F_PHI, vs.w);
-    put1(SPHGPU_F_NEIGHBOR, (double)S.nbr[i]);
+    // a record is read only when one of its fields is requested, so a
+    // download of some fields may overlap kernels that write the others
+    auto want = [&](int f0, int k) {
+        for(int f = f0; f < f0 + k; ++f)
+            if(F.p[f]) return true;
+        return false;
+    };
+    auto put4 = [&](int f0, const double4* rec, int fw) {
+        if(!want(f0, 3) && !F.p[fw]) return;
+        const double4 v = rec[i];
+        put1(f0, v.x);
+        put1(f0 + 1, v.y);
+        put1(f0 + 2, v.z);
+        put1(fw, v.w);
+    };
+    put4(SPHGPU_F_POS_X, S.pos, SPHGPU_F_MASS);
+    put4(SPHGPU_F_VEL_X, S.vel, SPHGPU_F_SML);
+    put4(SPHGPU_F_ACC_X, S.acc, SPHGPU_F_DENE);
+    put4(SPHGPU_F_VELP_X, S.velp, SPHGPU_F_ENE_P);
+    if(want(SPHGPU_F_DENS, 1) || want(SPHGPU_F_PRES, 1) || want(SPHGPU_F_ENE, 1) || want(SPHGPU_F_SOUND, 1)) {
+        const double4 th = S.thermo[i];
+        put1(SPHGPU_F_DENS, th.x);
+        put1(SPHGPU_F_PRES, th.y);
+        put1(SPHGPU_F_ENE, th.z);
+        put1(SPHGPU_F_SOUND, th.w);
+    }
+    if(want(SPHGPU_F_ALPHA, 1) || want(SPHGPU_F_BALSARA, 1) || want(SPHGPU_F_GRADH, 1) || want(SPHGPU_F_PHI, 1)) {
+        const double4 vs = S.visc[i];
+        put1(SPHGPU_F_ALPHA, vs.x);
+        put1(SPHGPU_F_BALSARA, vs.y);
+        put1(SPHGPU_F_GRADH, vs.z);
+        put1(SPHGPU_F_PHI, vs.w);
+    }
+    if(F.p[SPHGPU_F_NEIGHBOR]) put1(SPHGPU_F_NEIGHBOR, (double)S.nbr[i]);
     const size_t m = (size_t)n;
     for(int q = 0; q < 4; ++q) {
         const int f = SPHGPU_F_GRAD_D_X + 4 * q;
+        if(!want(f, q < 3 ? 4 : 3)) continue;
         const double4 v = S.grad[q * m + i];
         put1(f, v.x);
         put1(f + 1, v.y);
@@ -371,6 +382,7 @@ __global__ void k_get_all(DevState S, FieldSlots F, int n)
     if(S.sr) {
         for(int q = 0; q < 3; ++q) {
             const int f = SPHGPU_F_SR_S_X + 4 * q;
+            if(!want(f, 4)) continue;
             const double4 v = S.sr[q * m + i];
             put1(f, v.x);
             put1(f + 1, v.y);
@@ -525,6 +537,13 @@ int sphgpu_destroy(sphgpu_ctx* c)
 {
     if(!c) return SPHGPU_OK;
     if(c->stream) cudaStreamSynchronize(c->stream);
+    if(c->copy_stream) {
+        cudaStreamSynchronize(c->copy_stream);
+        cudaStreamDestroy(c->copy_stream);
+        for(cudaEvent_t e : c->copy_ev) {
+            if(e) cudaEventDestroy(e);
+        }
+    }
     free_all(c);
     if(c->d_mlp) cudaFree(c->d_mlp);
     if(c->d_mlp_master) cudaFree(c->d_mlp_master);
@@ -549,7 +568,11 @@ int sphgpu_destroy(sphgpu_ctx* c)
 
 const char* sphgpu_last_error(const sphgpu_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
-int sphgpu_upload(sphgpu_ctx* c, int64_t n, const double* const* fields)
+namespace {
+
+// sphgpu_upload; step = true (sphgpu_integrate_host) keeps the simulation
+// time and the initial-smoothing flag: the fields continue a run
+int upload_impl(sphgpu_ctx* c, int64_t n, const double* const* fields, bool step)
 {
     if(!c || n <= 0 || n > SPHGPU_MAX_PARTICLES)
         return fail(c, SPHGPU_ERR_ARG, "particle count out of range (1 .. SPHGPU_MAX_PARTICLES)");
@@ -585,9 +608,18 @@ int sphgpu_upload(sphgpu_ctx* c, int64_t n, const double* const* fields)
     SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
     c->have_tree = false;
     c->flist_ready = false;
-    c->first_pre = true;
-    c->time = 0.0;
+    if(!step) {
+        c->first_pre = true;
+        c->time = 0.0;
+    }
     return SPHGPU_OK;
+}
+
+}  // namespace
+
+int sphgpu_upload(sphgpu_ctx* c, int64_t n, const double* const* fields)
+{
+    return upload_impl(c, n, fields, false);
 }
 
 int sphgpu_download(sphgpu_ctx* c, double* const* fields)
@@ -784,6 +816,98 @@ int sphgpu_integrate(sphgpu_ctx* c)
     rc = sync_and_check(c);
     stage_flush(c);
     if(rc < 0) return rc;
+    c->time += dt_h;
+    return SPHGPU_OK;
+}
+
+namespace {
+
+// Fields of `out` in group g (0: final after tree_make: positions and mass,
+// which only predict moves; 1: final after PreInteraction; 2: the rest, final
+// after correct) packed into staging slots from *slot on, and copied to the
+// host on stream st.
+int download_group(sphgpu_ctx* c, double* const* out, int g, int* slot, cudaStream_t st)
+{
+    auto group_of = [](int f) {
+        if(f == SPHGPU_F_POS_X || f == SPHGPU_F_POS_Y || f == SPHGPU_F_POS_Z || f == SPHGPU_F_MASS) return 0;
+        if(f == SPHGPU_F_DENS || f == SPHGPU_F_PRES || f == SPHGPU_F_SML || f == SPHGPU_F_GRADH ||
+           f == SPHGPU_F_BALSARA || f == SPHGPU_F_ALPHA || f == SPHGPU_F_NEIGHBOR)
+            return 1;
+        return 2;
+    };
+    const int n = c->n;
+    FieldSlots F{};
+    bool any = false;
+    for(int f = 0; f < SPHGPU_NFIELDS; ++f) {
+        if(!out[f] || group_of(f) != g || (f >= SPHGPU_F_SR_S_X && !c->s.sr)) continue;
+        F.p[f] = c->d_stage + (size_t)(*slot)++ * (size_t)n;
+        any = true;
+    }
+    if(!any) return SPHGPU_OK;
+    k_get_all<<<grid_for(n, 256), 256, 0, st>>>(c->s, F, n);
+    SPHGPU_LAUNCH_CHECK(c, "integrate_host download");
+    for(int f = 0; f < SPHGPU_NFIELDS; ++f) {
+        if(!F.p[f]) continue;
+        SPHGPU_CUDA(c, cudaMemcpyAsync(out[f], F.p[f], sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, st));
+    }
+    return SPHGPU_OK;
+}
+
+// After event ev on the step's stream, the group's download on the copy stream.
+int download_group_after(sphgpu_ctx* c, double* const* out, int g, int* slot, cudaEvent_t ev)
+{
+    SPHGPU_CUDA(c, cudaEventRecord(ev, c->stream));
+    SPHGPU_CUDA(c, cudaStreamWaitEvent(c->copy_stream, ev, 0));
+    return download_group(c, out, g, slot, c->copy_stream);
+}
+
+int integrate_host_step(sphgpu_ctx* c, double* const* out, double* dt_h)
+{
+    int rc, slot = 0;
+    if((rc = timestep(c)) < 0) return rc;
+    SPHGPU_CUDA(c, cudaMemcpyAsync(dt_h, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if((rc = predict(c)) < 0) return rc;
+    if((rc = tree_make(c)) < 0) return rc;
+    if((rc = download_group_after(c, out, 0, &slot, c->copy_ev[0])) < 0) return rc;
+    if((rc = pre_interaction(c)) < 0) return rc;
+    if((rc = download_group_after(c, out, 1, &slot, c->copy_ev[1])) < 0) return rc;
+    if((rc = fluid_force(c)) < 0) return rc;
+    if((rc = gravity(c, false)) < 0) return rc;
+    if((rc = correct(c)) < 0) return rc;
+    return download_group(c, out, 2, &slot, c->stream);
+}
+
+}  // namespace
+
+int sphgpu_integrate_host(sphgpu_ctx* c, const double* const* in_fields, double* const* out_fields)
+{
+    SPHGPU_NEED_STATE(c);
+    if(!in_fields || !out_fields) return fail(c, SPHGPU_ERR_ARG, "integrate_host: field tables required");
+    if(!c->copy_stream) {
+        SPHGPU_CUDA(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        for(cudaEvent_t& e : c->copy_ev) SPHGPU_CUDA(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    int in_slots = 0, out_slots = 0;
+    for(int f = 0; f < SPHGPU_NFIELDS; ++f) {
+        const bool kept = f < SPHGPU_F_SR_S_X || c->s.sr;
+        in_slots += in_fields[f] && kept ? 1 : 0;
+        out_slots += out_fields[f] && kept ? 1 : 0;
+    }
+    int rc = ensure_stage(c, std::max(in_slots, out_slots));
+    if(rc) return rc;
+    if((rc = upload_impl(c, c->n, in_fields, true)) < 0) return rc;
+    double dt_h = 0.0;
+    rc = integrate_host_step(c, out_fields, &dt_h);
+    // both streams drain on every path: no copy into the caller's buffers
+    // outlives the call
+    const cudaError_t e1 = cudaStreamSynchronize(c->copy_stream);
+    const int rs = sync_and_check(c);
+    stage_flush(c);
+    if(rc < 0) return rc;
+    if(rs < 0) return rs;
+    if(e1 != cudaSuccess) return fail(c, SPHGPU_ERR_CUDA, cudaGetErrorString(e1));
+    for(int f = SPHGPU_F_SR_S_X; f < SPHGPU_NFIELDS; ++f)
+        if(out_fields[f] && !c->s.sr) std::fill(out_fields[f], out_fields[f] + c->n, 0.0);
     c->time += dt_h;
     return SPHGPU_OK;
 }

@@ -134,6 +134,7 @@ def lib() -> C.CDLL:
         "sphgpu_correct": (C.c_int, [vp]),
         "sphgpu_initialize": (C.c_int, [vp]),
         "sphgpu_integrate": (C.c_int, [vp]),
+        "sphgpu_integrate_host": (C.c_int, [vp, dpp, dpp]),
         "sphgpu_energies": (C.c_int, [vp, dp, dp, dp, dp]),
         "sphgpu_write_csv": (C.c_int, [vp, C.c_char_p, C.c_int, C.c_int]),
         "sphgpu_relax_step": (C.c_int, [vp, C.POINTER(LaneEmden), C.c_int, dp]),
@@ -363,6 +364,17 @@ class Simulation:
 
     def integrate(self):
         return self._check(lib().sphgpu_integrate(self._h), "integrate")
+
+    def integrate_host(self, fields: Dict[str, np.ndarray], out_names=None) -> Dict[str, np.ndarray]:
+        """One step on host buffers (sphgpu_integrate_host): `fields` replace
+        the device state, the step runs, the named fields come back."""
+        names = list(FIELDS) if out_names is None else list(out_names)
+        ptrs_in, keep = _field_ptrs({k: v for k, v in fields.items() if k in FIELD_INDEX}, self.n, False)
+        out = {f: np.zeros(self.n) for f in names}
+        ptrs_out, _ = _field_ptrs(out, self.n, True)
+        self._check(lib().sphgpu_integrate_host(self._h, ptrs_in, ptrs_out), "integrate_host")
+        del keep
+        return out
 
     def energies(self):
         k, u, w = C.c_double(), C.c_double(), C.c_double()
