@@ -276,15 +276,21 @@ __global__ void __launch_bounds__(FBLK, (force_min_blocks<T, TYPE>())) k_force(D
         double ax = 0, ay = 0, az = 0, de = 0;
         float sabs = 0.f;  // mixed form: sum of |FP32 force terms|, the rounding-error scale
         n_cand += lane < cnt ? (unsigned)((cnt - lane + G - 1) / G) : 0u;
+        // the next pair's index is fetched one iteration ahead, so the
+        // neighbour's loads do not wait on the list load
+        int jn = MODE != 4 && lane < cnt ? __ldg(&li[lane]) : 0;
         for(int k = lane; k < cnt; k += G) {
             float yq = 0.f;
-            int kk = k;
+            int j;
             if(MODE == 4) {
                 const int row = mp.dstart[i] + k;
-                kk = (int)(mp.skeys[row] - (uint64_t)i * (uint64_t)cap);
+                const int kk = (int)(mp.skeys[row] - (uint64_t)i * (uint64_t)cap);
                 yq = mp.y[mp.svals[row]];
+                j = li[kk];
+            } else {
+                j = jn;
+                if(k + G < cnt) jn = __ldg(&li[k + G]);
             }
-            const int j = li[kk];
             const double4 pj = ldg4(&S.pos[j]);
             const Vec3d d = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
             const double4 vj = ldg4(&S.vel[j]);

@@ -118,14 +118,7 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
                 T d = 0, dd = 0;
                 const KernH<T> kh(P.kernel, (T)h);
                 const bool exact = skin_delta > 0.0 && !(h < sml0 - skin_delta);
-                // the next candidate's index is fetched one iteration ahead,
-                // so the position load does not wait on the list load
-                int jn = lane < cnt ? __ldg(&li[lane]) : 0;
-                n_cand += lane < cnt ? (unsigned)((cnt - lane + G - 1) / G) : 0u;
-                for(int k = lane; k < cnt; k += G) {
-                    const int jc = jn;
-                    if(k + G < cnt) jn = __ldg(&li[k + G]);
-                    const double4 pj = ldg4(&S.pos[jc]);
+                auto visit = [&](const double4& pj, int jc) {
                     const double r2 = abs2x(rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z));
                     T rT;
                     if(sweep_r(r2, h, rT) && (!exact || gather_member(P, Tr, pi.x, pi.y, pi.z, sml0, skin_delta, jc, r2))) {
@@ -140,6 +133,23 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
                             dd += (T)pj.w * dh;
                         }
                     }
+                };
+                // two candidates per iteration (the same per-lane order), their
+                // indices fetched an iteration ahead: two position loads in
+                // flight, neither waiting on the list load (8.78 M sphere:
+                // 34.9 -> 32.5 ms FP64)
+                int ja = lane < cnt ? __ldg(&li[lane]) : 0;
+                int jb = lane + G < cnt ? __ldg(&li[lane + G]) : 0;
+                n_cand += lane < cnt ? (unsigned)((cnt - lane + G - 1) / G) : 0u;
+                for(int k = lane; k < cnt; k += 2 * G) {
+                    const int ca = ja, cb = jb;  // cb is a valid index even past the list end
+                    const bool two = k + G < cnt;
+                    if(k + 2 * G < cnt) ja = __ldg(&li[k + 2 * G]);
+                    if(k + 3 * G < cnt) jb = __ldg(&li[k + 3 * G]);
+                    const double4 pa = ldg4(&S.pos[ca]);
+                    const double4 pb = ldg4(&S.pos[cb]);
+                    visit(pa, ca);
+                    if(two) visit(pb, cb);
                 }
                 const double ds = (double)group_sum<G>(d), dds = (double)group_sum<G>(dd);
                 const double h3 = h * h * h;
@@ -167,27 +177,23 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
         const bool need_av = !gsph && (P.balsara || P.td_av);
         const bool need_grad = (gsph || gdisph) && P.gsph2;
         const bool exact = skin_delta > 0.0 && !(h < sml0 - skin_delta);
-        int jn2 = lane < cnt ? __ldg(&li[lane]) : 0;
         n_cand += lane < cnt ? (unsigned)((cnt - lane + G - 1) / G) : 0u;
         n_list += lane < cnt ? (unsigned)((cnt - lane + G - 1) / G) : 0u;
-        for(int k = lane; k < cnt; k += G) {
-            const int j = jn2;
-            if(k + G < cnt) jn2 = __ldg(&li[k + G]);
-            const double4 pj = ldg4(&S.pos[j]);
+        auto visit = [&](const double4& pj, int j) {
             const Vec3d dv = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
             const double r2 = abs2x(dv);
             double r, rinv;
             if constexpr(sizeof(T) == sizeof(float)) {
                 // the set predicate in FP64, the distance in FP32 (mixed form)
-                if(!root_lt(r2, h)) continue;
+                if(!root_lt(r2, h)) return;
                 const float r2f = (float)r2;
                 const float rif = r2f > 0.f ? rsqrtf(r2f) : 0.f;
                 r = (double)(r2f * rif);
                 rinv = (double)rif;
             } else {
-                if(!pair_within(r2, h, r, rinv)) continue;
+                if(!pair_within(r2, h, r, rinv)) return;
             }
-            if(exact && !gather_member(P, Tr, pi.x, pi.y, pi.z, sml0, skin_delta, j, r2)) continue;
+            if(exact && !gather_member(P, Tr, pi.x, pi.y, pi.z, sml0, skin_delta, j, r2)) return;
             ++nn;
             // neighbours' velocities and u, c_s: components no thread here writes
             const double4 vj = ldg4(&S.vel[j]);
@@ -246,6 +252,31 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
                     gv[7] += dwy * m2;
                     gv[8] += dwz * m2;
                 }
+            }
+        };
+        if constexpr(sizeof(T) == sizeof(double) && TYPE == SPHGPU_DISPH) {
+            // two candidates per iteration, as in the sweep (8.78 M sphere
+            // 32.4 -> 31.7 ms; slower for the other instantiations, whose
+            // larger bodies then spill)
+            int ja = lane < cnt ? __ldg(&li[lane]) : 0;
+            int jb = lane + G < cnt ? __ldg(&li[lane + G]) : 0;
+            for(int k = lane; k < cnt; k += 2 * G) {
+                const int ca = ja, cb = jb;  // cb is a valid index even past the list end
+                const bool two = k + G < cnt;
+                if(k + 2 * G < cnt) ja = __ldg(&li[k + 2 * G]);
+                if(k + 3 * G < cnt) jb = __ldg(&li[k + 3 * G]);
+                const double4 pa = ldg4(&S.pos[ca]);
+                const double4 pb = ldg4(&S.pos[cb]);
+                visit(pa, ca);
+                if(two) visit(pb, cb);
+            }
+        } else {
+            // the next candidate's index is fetched one iteration ahead
+            int jn = lane < cnt ? __ldg(&li[lane]) : 0;
+            for(int k = lane; k < cnt; k += G) {
+                const int j = jn;
+                if(k + G < cnt) jn = __ldg(&li[k + G]);
+                visit(ldg4(&S.pos[j]), j);
             }
         }
         n_pairs += (unsigned)nn;
