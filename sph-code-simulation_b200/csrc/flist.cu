@@ -69,31 +69,41 @@ __global__ void __launch_bounds__(LBLK, 6) k_flist(DevParams P, DevState S, int 
         const int* li = glist + (size_t)i * (size_t)gcap;
         int* row = plist + (size_t)i * (size_t)pcap;
         int oc = 0;
-        for(int kk = 0; kk < cnt; kk += G) {
-            const int k = kk + lane;
-            bool own = false;
-            int j = 0;
-            if(k < cnt) {
-                j = __ldg(&li[k]);
-                const double4 pj = ldg4(&S.pos[j]);
-                const Vec3d d = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
-                const double r2 = abs2x(d);
-                const double r = sqrt(r2);
-                if(r < hi && (!exact || gather_member(P, Tr, pi.x, pi.y, pi.z, ri, skin_delta, j, r2))) {
-                    own = true;
-                    if(!(r < __ldg(&S.vel[j].w))) {
-                        // j's own scan does not reach i: append i to j's row
-                        const int t = atomicAdd(&tcount[j], 1);
-                        if(t < pcap) plist[(size_t)j * (size_t)pcap + (pcap - 1 - t)] = i;
-                    }
-                }
+        // r < h_i (an own pair) and, for an own pair j's kernel not reaching
+        // i, the entry appended to j's row
+        auto test = [&](int j, const double4& pj) {
+            const Vec3d d = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
+            const double r2 = abs2x(d);
+            const double r = sqrt(r2);
+            if(!(r < hi && (!exact || gather_member(P, Tr, pi.x, pi.y, pi.z, ri, skin_delta, j, r2)))) return false;
+            if(!(r < __ldg(&S.vel[j].w))) {
+                const int t = atomicAdd(&tcount[j], 1);
+                if(t < pcap) plist[(size_t)j * (size_t)pcap + (pcap - 1 - t)] = i;
             }
+            return true;
+        };
+        auto compact = [&](bool own, int j) {
             const unsigned m = (__ballot_sync(gmask, own) >> gbase) & ((1u << G) - 1u);
             if(own) {
                 const int pos = oc + __popc(m & ((1u << lane) - 1u));
                 if(pos < pcap) row[pos] = j;
             }
             oc += __popc(m);
+        };
+        // two chunks of G entries per iteration, their indices fetched an
+        // iteration ahead: two position loads per lane in flight (8.78 M
+        // sphere 16.6 -> 15.9 ms; 1 M shear layer 1.73 -> 1.81 ms)
+        int ja = lane < cnt ? __ldg(&li[lane]) : 0;
+        int jb = G + lane < cnt ? __ldg(&li[G + lane]) : 0;
+        for(int kk = 0; kk < cnt; kk += 2 * G) {
+            const int ca = ja, cb = jb;  // valid indices even past the list end
+            const bool ina = kk + lane < cnt, inb = kk + G + lane < cnt;
+            if(kk + 2 * G + lane < cnt) ja = __ldg(&li[kk + 2 * G + lane]);
+            if(kk + 3 * G + lane < cnt) jb = __ldg(&li[kk + 3 * G + lane]);
+            const double4 pa = ldg4(&S.pos[ca]);
+            const double4 pb = ldg4(&S.pos[cb]);
+            compact(ina && test(ca, pa), ca);
+            compact(inb && test(cb, pb), cb);
         }
         if(lane == 0) pcount[i] = oc;
     }
