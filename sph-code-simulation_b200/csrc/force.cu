@@ -210,11 +210,13 @@ __device__ void riemann_iterative(const double* L, const double* R, double gamma
 // deferred pairs only, with the network's guess, added to acc.
 // Minimum resident blocks per SM (caps registers; measured on B200): FP64
 // disph 2 (27.2 -> 24.5 ms on the 8.78 M sphere), FP64 gdisph 3 (8.8 -> 7.7 ms
-// on the 2 M tube), gsph and the FP32 forms 4 (gsph 18.8 -> 9.6 ms against 3;
-// FP32 disph 17.2 against 17.5 ms with 3), FP64 ssph 3.
+// on the 2 M tube), FP32 disph 3 (17.3 -> 16.0 ms, once the next pair's index
+// is fetched ahead), gsph and the other FP32 forms 4 (gsph 18.8 -> 9.6 ms
+// against 3), FP64 ssph 3.
 template <typename T, int TYPE>
 constexpr int force_min_blocks()
 {
+    if(sizeof(T) == sizeof(float) && TYPE == SPHGPU_DISPH) return 3;
     if(sizeof(T) == sizeof(float) || TYPE == SPHGPU_GSPH) return 4;
     return TYPE == SPHGPU_DISPH ? 2 : 3;
 }
