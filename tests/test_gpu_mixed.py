@@ -8,9 +8,9 @@ state.  Measured on B200 (one FluidForce + GravityForce from the same state):
 
 | workload | density | acceleration |
 |---|---|---|
-| disph Evrard sphere 137 K (config 4's set-up) | 6e-8 | 1.7e-7 (met) |
-| disph shear layer 130 K (config 1) | 7e-8 | 2.6e-3 (missed) |
-| gsph shock tube 250 K (config 2) | 2e-8 | ill-defined: ahead of the shock |a| is 1e-20 of max|a| |
+| disph Evrard sphere 137 K (config 4's set-up) | 7e-8 | 1.9e-7 (met) |
+| disph shear layer 130 K (config 1) | 8e-8 | 3.0e-3 (missed) |
+| gsph shock tube 250 K (config 2) | 1.4e-7 | ill-defined: ahead of the shock |a| is 1e-20 of max|a| |
 
 In the shear layer's pressure-balanced bulk the acceleration is a residue
 1e-3 .. 1e-6 of the cancelling pair terms; the FP32 density and pressure the
