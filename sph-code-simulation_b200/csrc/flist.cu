@@ -44,8 +44,10 @@ __global__ void k_save_radius(const DevState S, int n, double* __restrict__ rs)
     if(i < n) rs[i] = S.vel[i].w;
 }
 
+// 5 resident blocks (48 registers): 15.8 -> 14.5 ms against 6 on the 8.78 M
+// sphere, 1.81 -> 1.69 ms on the 1 M shear layer (4 is slower)
 template <int G>
-__global__ void __launch_bounds__(LBLK, 6) k_flist(DevParams P, DevState S, int n, const int* __restrict__ glist,
+__global__ void __launch_bounds__(LBLK, 5) k_flist(DevParams P, DevState S, int n, const int* __restrict__ glist,
                                                 const int* __restrict__ gcount, int gcap,
                                                 const double* __restrict__ rs, int* __restrict__ plist,
                                                 int* __restrict__ pcount, int* __restrict__ tcount, int pcap,
