@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(WBLK) k_walk(DevParams P, DevState S, DevTree 
 // superset of the reference's candidates gives the same lists, because the
 // per-pair classification alone decides membership.  A stack overflow marks
 // the warp and the host re-runs the call with the per-lane walk.
-constexpr int GW_WARPS = 4;
+constexpr int GW_WARPS = 2;  // warps per block (2: 1 M shear walk 4.38 -> 4.14 ms against 4; 1: 4.33)
 constexpr int GW_STACK = 1024;
 constexpr int GW_QUEUE = 64;
 constexpr int GW_WHOLE = 8;   // nodes with at most this many particles are queued whole
