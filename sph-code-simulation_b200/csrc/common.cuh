@@ -141,7 +141,8 @@ constexpr int PASS_GUARD_GRAVITY32 = 8;  // Barnes-Hut walk (mixed form)
 // Read-only 32-byte load through the non-coherent path, one 256-bit access
 // (sm_100).  p must be 32-byte aligned: every double4 array here is an
 // allocation of its own (256-byte aligned) indexed by element.  Only for data
-// that no thread of the kernel writes, or whose read components it does not.
+// that no thread of the kernel writes (the non-coherent path may return an
+// older value of a location written during the kernel).
 __device__ __forceinline__ double4 ldg4(const double4* p)
 {
     double4 r;

@@ -195,9 +195,11 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
             }
             if(exact && !gather_member(P, Tr, pi.x, pi.y, pi.z, sml0, skin_delta, j, r2)) return;
             ++nn;
-            // neighbours' velocities and u, c_s: components no thread here writes
-            const double4 vj = ldg4(&S.vel[j]);
-            const double4 tj = ldg4(&S.thermo[j]);
+            // coherent loads: this kernel writes vel.w and thermo.x, .y of every
+            // particle (the components read here, velocity, u and c_s, it
+            // does not change)
+            const double4 vj = S.vel[j];
+            const double4 tj = S.thermo[j];
             const T rT = (T)r;
             const T w = kh.w(rT);
             const T mj = (T)pj.w;
