@@ -799,6 +799,8 @@ double skin_delta(sphgpu_ctx* c)
     return 1e-12 * (std::max(std::fabs(root.x), std::max(std::fabs(root.y), std::fabs(root.z))) + root.w);
 }
 
+// Returns SPHGPU_OK, a CUDA failure (< 0), or 1 when the device has no room
+// for the skin buffers (the caller then walks exactly instead).
 int skin_alloc(sphgpu_ctx* c)
 {
     // per-particle arrays (build radius and position, counts, permutation
@@ -806,6 +808,12 @@ int skin_alloc(sphgpu_ctx* c)
     // an allocation of its own: it trades places with d_glist at every
     // permutation
     const size_t n = (size_t)c->n;
+    auto room = [&](void** p, size_t bytes) {
+        if(cudaMalloc(p, bytes) == cudaSuccess) return true;
+        (void)cudaGetLastError();  // an allocation failure is not sticky: clear it
+        *p = nullptr;
+        return false;
+    };
     if(c->skin_n != c->n || !c->d_skin) {
         if(c->d_skin) {
             SPHGPU_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -814,7 +822,8 @@ int skin_alloc(sphgpu_ctx* c)
         }
         auto al = [](size_t b) { return (b + 255) / 256 * 256; };
         const size_t bytes = al(4 * n) + 2 * al(8 * n) + 2 * al(32 * n) + 3 * al(4 * n) + 256;
-        SPHGPU_CUDA(c, cudaMalloc(&c->d_skin, bytes));
+        c->skin_n = 0;
+        if(!room(&c->d_skin, bytes)) return 1;
         char* b = static_cast<char*>(c->d_skin);
         size_t off = 0;
         auto take = [&](size_t sz) {
@@ -841,7 +850,8 @@ int skin_alloc(sphgpu_ctx* c)
             SPHGPU_CUDA(c, cudaFree(c->d_glist_alt));
             c->d_glist_alt = nullptr;
         }
-        SPHGPU_CUDA(c, cudaMalloc(&c->d_glist_alt, std::max<size_t>(4 * n * (size_t)c->gcap, 4)));
+        c->skin_cap = 0;
+        if(!room(reinterpret_cast<void**>(&c->d_glist_alt), std::max<size_t>(4 * n * (size_t)c->gcap, 4))) return 1;
         c->skin_cap = c->gcap;
     }
     return SPHGPU_OK;
@@ -937,6 +947,12 @@ int gather_lists(sphgpu_ctx* c, double ratio)
     if(rc < 0) return rc;
     rc = skin_alloc(c);
     if(rc < 0) return rc;
+    if(rc == 1) {
+        // no room for a second list buffer: exact walks from here on
+        c->skin_valid = false;
+        c->skin_off = 1 << 30;
+        return gather_walk(c, true, ratio);
+    }
     c->skin_valid = false;
     stage_begin(c, SPHGPU_T_GATHER_WALK);
     int launches = 0;
@@ -948,6 +964,12 @@ int gather_lists(sphgpu_ctx* c, double ratio)
     // follows (the recorded radii and positions are per particle and stand)
     const int ra = skin_alloc(c);
     if(ra < 0) return ra;
+    if(ra == 1) {
+        // the grown lists leave no room for their second buffer: these lists
+        // are skin lists (supersets) and must not be taken as exact ones
+        c->skin_off = 1 << 30;
+        return gather_walk(c, true, ratio);
+    }
     c->skin_valid = true;
     c->skin_built = true;
     ++c->skin_builds;
