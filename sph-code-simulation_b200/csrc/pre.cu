@@ -12,7 +12,8 @@
 // that mostly hit L1/L2 because neighbours are close in octree order).
 //   1. Newton-Raphson on h (<= 10 iterations, |dh| < 1e-4 (h + h_b)) over the
 //      candidates with r < h, group-reduced each iteration;
-//   2. one fused pass at the final h: density (and the DISPH number/pressure
+//   2. one fused pass at the final h (disph: over the candidates the last
+//      sweep kept, within (1 + 4e-4) of its h): density (and the DISPH number/pressure
 //      sums), grad-h sums, max signal speed, neighbour count, the Balsara
 //      div/curl sums and the GSPH MUSCL gradients — every quantity the
 //      reference computes in separate loops over the same set {r < h};
@@ -80,7 +81,7 @@ template <typename T, int G, int TYPE>
 __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevParams P, DevState S, int n, const int* __restrict__ list,
                                               const int* __restrict__ count, int cap, const double* __restrict__ dtp,
                                               double* __restrict__ hvs, DevStatus* __restrict__ st, DevTree Tr,
-                                              double skin_delta)
+                                              double skin_delta, int* __restrict__ scratch, int scap)
 {
     constexpr int GPW = 32 / G;
     const int lane = threadIdx.x & (G - 1);
@@ -109,17 +110,32 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
         // ---- 1. smoothing length (src/pre_interaction.cpp:227-283,
         //         src/disph/d_pre_interaction.cpp:174-230)
         double h = sml0;
+        // disph: each sweep also keeps, per lane and in the lane's own order,
+        // the candidates within (1 + 4e-4) h in a scratch row; after a
+        // converged sweep (|h_new - h| < 1e-4 (h_new + h), so h_new <
+        // (1 + 2.0003e-4) h) they hold every pair of the fused pass, which
+        // then reads them instead of the whole list (8.78 M sphere: pre 31.8
+        // -> 30.8 ms FP64, 27.4 -> 24.1 ms FP32; the gsph and gdisph bodies
+        // spill with it and run slower)
+        constexpr bool keep = TYPE == SPHGPU_DISPH;
+        int* srow = scratch + (size_t)(valid ? i : 0) * (size_t)scap;
+        int nk = 0;
+        bool conv = false;
         if(P.iterative) {
             h = sml0 / P.ratio;
             const double b = disph ? P.nngb / AREA3 : pi.w * P.nngb / AREA3;
-            bool conv = false;
             for(int it = 0; it < 10; ++it) {
                 const double hb = h;
                 T d = 0, dd = 0;
                 const KernH<T> kh(P.kernel, (T)h);
                 const bool exact = skin_delta > 0.0 && !(h < sml0 - skin_delta);
+                const double hk = h * (1.0 + 4e-4), keep2 = hk * hk;
+                nk = 0;
                 auto visit = [&](const double4& pj, int jc) {
                     const double r2 = abs2x(rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z));
+                    if constexpr(keep) {
+                        if(r2 < keep2) srow[lane + G * nk++] = jc;
+                    }
                     T rT;
                     if(sweep_r(r2, h, rT) && (!exact || gather_member(P, Tr, pi.x, pi.y, pi.z, sml0, skin_delta, jc, r2))) {
                         ++n_newton;
@@ -177,8 +193,9 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
         const bool need_av = !gsph && (P.balsara || P.td_av);
         const bool need_grad = (gsph || gdisph) && P.gsph2;
         const bool exact = skin_delta > 0.0 && !(h < sml0 - skin_delta);
-        n_cand += lane < cnt ? (unsigned)((cnt - lane + G - 1) / G) : 0u;
         n_list += lane < cnt ? (unsigned)((cnt - lane + G - 1) / G) : 0u;
+        const bool kept = keep && conv;
+        n_cand += kept ? (unsigned)nk : (lane < cnt ? (unsigned)((cnt - lane + G - 1) / G) : 0u);
         auto visit = [&](const double4& pj, int j) {
             const Vec3d dv = rij(P, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z);
             const double r2 = abs2x(dv);
@@ -256,7 +273,21 @@ __global__ void __launch_bounds__(PBLK, (pre_min_blocks<T, TYPE>())) k_pre(DevPa
                 }
             }
         };
-        if constexpr(sizeof(T) == sizeof(double) && TYPE == SPHGPU_DISPH) {
+        if(kept) {
+            // the lane's kept candidates, in its own order (the same sums)
+            int m = 0;
+            for(; m + 1 < nk; m += 2) {
+                const int ca = srow[lane + G * m], cb = srow[lane + G * (m + 1)];
+                const double4 pa = ldg4(&S.pos[ca]);
+                const double4 pb = ldg4(&S.pos[cb]);
+                visit(pa, ca);
+                visit(pb, cb);
+            }
+            if(m < nk) {
+                const int ca = srow[lane + G * m];
+                visit(ldg4(&S.pos[ca]), ca);
+            }
+        } else if constexpr(sizeof(T) == sizeof(double) && TYPE == SPHGPU_DISPH) {
             // two candidates per iteration, as in the sweep (8.78 M sphere
             // 32.4 -> 31.7 ms; slower for the other instantiations, whose
             // larger bodies then spill)
@@ -460,16 +491,20 @@ void launch_pre(sphgpu_ctx* c)
     const int type = c->prm.sph_type;
     if(type == SPHGPU_DISPH) {
         k_pre<T, GROUP, SPHGPU_DISPH><<<grid, PBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_glist, c->d_gcount,
-                                                                    (int)c->gcap, c->d_dt, c->d_hvs, c->d_status, c->t, sd);
+                                                                    (int)c->gcap, c->d_dt, c->d_hvs, c->d_status, c->t, sd,
+                                                                   c->d_plist, (int)c->pcap);
     } else if(type == SPHGPU_GSPH) {
         k_pre<T, GROUP, SPHGPU_GSPH><<<grid, PBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_glist, c->d_gcount,
-                                                                   (int)c->gcap, c->d_dt, c->d_hvs, c->d_status, c->t, sd);
+                                                                   (int)c->gcap, c->d_dt, c->d_hvs, c->d_status, c->t, sd,
+                                                                   c->d_plist, (int)c->pcap);
     } else if(type == SPHGPU_GDISPH) {
         k_pre<T, GROUP, SPHGPU_GDISPH><<<grid, PBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_glist, c->d_gcount,
-                                                                     (int)c->gcap, c->d_dt, c->d_hvs, c->d_status, c->t, sd);
+                                                                     (int)c->gcap, c->d_dt, c->d_hvs, c->d_status, c->t, sd,
+                                                                   c->d_plist, (int)c->pcap);
     } else {
         k_pre<T, GROUP, SPHGPU_SSPH><<<grid, PBLK, 0, c->stream>>>(c->dp, c->s, c->n, c->d_glist, c->d_gcount,
-                                                                   (int)c->gcap, c->d_dt, c->d_hvs, c->d_status, c->t, sd);
+                                                                   (int)c->gcap, c->d_dt, c->d_hvs, c->d_status, c->t, sd,
+                                                                   c->d_plist, (int)c->pcap);
     }
 }
 
@@ -501,6 +536,8 @@ int pre_interaction(sphgpu_ctx* c)
     if(rc_walk < 0) return rc_walk;
     int rcs = save_gather_radius(c);
     if(rcs < 0) return rcs;
+    // the pair-list buffer is the sweeps' scratch (the pair lists are built after)
+    if(c->pcap < c->gcap && (rcs = ensure_list_capacity(c, 1, c->gcap)) < 0) return rcs;
     stage_begin(c, SPHGPU_T_PRE);
     const double big = DBL_MAX;
     SPHGPU_CUDA(c, cudaMemcpyAsync(c->d_hvs, &big, sizeof(double), cudaMemcpyHostToDevice, c->stream));
