@@ -26,7 +26,10 @@
 // loop) was measured slower: shear 1 M pre + lists 7.1 ms against 4.8 + 1.7 ms.
 // So was letting the fused pass write only the own part (ballot compaction,
 // lanes kept in step for it) and this pass only the appended part: on the
-// 8.78 M sphere lists 15.9 -> 10.1 ms but pre 31.7 -> 44.8 ms.
+// 8.78 M sphere lists 15.9 -> 10.1 ms but pre 31.7 -> 44.8 ms.  Scanning the
+// candidates PreInteraction's last sweep kept within (1 + 4e-4) h (about
+// half the list) instead of the list: 14.4 -> 14.6 ms, no gain; the scan is
+// not what bounds this pass.
 #include <cuda_runtime.h>
 
 #include "context.cuh"
