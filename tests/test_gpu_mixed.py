@@ -2,7 +2,7 @@
 accumulators, kick-drift and set predicates) against the plain FP64 form and
 the FP64 oracle.
 
-The metric is the north star's: the median over particles of the relative
+The metric is the mixed form's accuracy criterion: the median over particles of the relative
 error |a_mixed - a| / |a| of the acceleration (and of the density), from one
 state.  Measured on B200 (one FluidForce + GravityForce from the same state):
 
@@ -110,7 +110,7 @@ def test_mixed_density_median_at_scale(scale_case):
 
 
 def test_mixed_acceleration_median_at_scale(request, scale_case):
-    """The north star's bar: median per-particle relative error <= 1e-5."""
+    """The accuracy bar: median per-particle relative error <= 1e-5."""
     name, ref, mixed, checked, _ = scale_case
     if not name.startswith("evrard"):
         request.applymarker(pytest.mark.xfail(strict=True, reason="missed: acceleration is a residue of cancelling "
