@@ -392,6 +392,21 @@ __global__ void k_get_all(DevState S, FieldSlots F, int n)
     }
 }
 
+// sphgpu_integrate_host: the alpha / Balsara / grad-h fields uploaded beside
+// the tree build, written once the particles are in tree order (slot by the
+// caller index each particle carries)
+__global__ void k_put_visc(DevState S, FieldSlots F, int n)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= n) return;
+    const int k = S.id[p];
+    double4 v = S.visc[p];
+    if(F.p[SPHGPU_F_ALPHA]) v.x = F.p[SPHGPU_F_ALPHA][k];
+    if(F.p[SPHGPU_F_BALSARA]) v.y = F.p[SPHGPU_F_BALSARA][k];
+    if(F.p[SPHGPU_F_GRADH]) v.z = F.p[SPHGPU_F_GRADH][k];
+    S.visc[p] = v;
+}
+
 // Staging for `slots` fields of n doubles, grown on demand and kept.
 int ensure_stage(sphgpu_ctx* c, int slots)
 {
@@ -861,13 +876,19 @@ int download_group_after(sphgpu_ctx* c, double* const* out, int g, int* slot, cu
     return download_group(c, out, g, slot, c->copy_stream);
 }
 
-int integrate_host_step(sphgpu_ctx* c, double* const* out, double* dt_h)
+int integrate_host_step(sphgpu_ctx* c, double* const* out, double* dt_h, const FieldSlots& late, bool has_late)
 {
     int rc, slot = 0;
     if((rc = timestep(c)) < 0) return rc;
     SPHGPU_CUDA(c, cudaMemcpyAsync(dt_h, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if((rc = predict(c)) < 0) return rc;
     if((rc = tree_make(c)) < 0) return rc;
+    if(has_late) {
+        // the fields PreInteraction reads first arrived beside the tree build
+        SPHGPU_CUDA(c, cudaStreamWaitEvent(c->stream, c->copy_ev[2], 0));
+        k_put_visc<<<grid_for(c->n, 256), 256, 0, c->stream>>>(c->s, late, c->n);
+        SPHGPU_LAUNCH_CHECK(c, "integrate_host late fields");
+    }
     if((rc = download_group_after(c, out, 0, &slot, c->copy_ev[0])) < 0) return rc;
     if((rc = pre_interaction(c)) < 0) return rc;
     if((rc = download_group_after(c, out, 1, &slot, c->copy_ev[1])) < 0) return rc;
@@ -895,9 +916,34 @@ int sphgpu_integrate_host(sphgpu_ctx* c, const double* const* in_fields, double*
     }
     int rc = ensure_stage(c, std::max(in_slots, out_slots));
     if(rc) return rc;
-    if((rc = upload_impl(c, c->n, in_fields, true)) < 0) return rc;
+    // alpha, Balsara and grad-h are first read by PreInteraction: they go up
+    // on the copy stream while the step's first modules run (srgsph contexts
+    // take every field before the step)
+    const int late_f[3] = {SPHGPU_F_ALPHA, SPHGPU_F_BALSARA, SPHGPU_F_GRADH};
+    const bool split = c->prm.sph_type != SPHGPU_SRGSPH;
+    const double* early[SPHGPU_NFIELDS];
+    for(int f = 0; f < SPHGPU_NFIELDS; ++f) early[f] = in_fields[f];
+    int n_late = 0;
+    if(split) {
+        for(int f : late_f) {
+            if(in_fields[f]) ++n_late;
+            early[f] = nullptr;
+        }
+    }
+    if((rc = upload_impl(c, c->n, early, true)) < 0) return rc;
+    FieldSlots late{};
+    if(n_late > 0) {
+        int k = in_slots - n_late;  // the slots after the early fields'
+        for(int f : late_f) {
+            if(!in_fields[f]) continue;
+            late.p[f] = c->d_stage + (size_t)k++ * (size_t)c->n;
+            SPHGPU_CUDA(c, cudaMemcpyAsync(late.p[f], in_fields[f], sizeof(double) * (size_t)c->n,
+                                           cudaMemcpyHostToDevice, c->copy_stream));
+        }
+        SPHGPU_CUDA(c, cudaEventRecord(c->copy_ev[2], c->copy_stream));
+    }
     double dt_h = 0.0;
-    rc = integrate_host_step(c, out_fields, &dt_h);
+    rc = integrate_host_step(c, out_fields, &dt_h, late, n_late > 0);
     // both streams drain on every path: no copy into the caller's buffers
     // outlives the call
     const cudaError_t e1 = cudaStreamSynchronize(c->copy_stream);

@@ -16,7 +16,7 @@ struct sphgpu_ctx {
     sphgpu::DevParams dp{};
     cudaStream_t stream = nullptr;
     cudaStream_t copy_stream = nullptr;  // sphgpu_integrate_host: downloads beside the step
-    cudaEvent_t copy_ev[2] = {};
+    cudaEvent_t copy_ev[3] = {};
     std::string err;
     int n = 0;
     bool have_tree = false;     // octree valid for the current positions
