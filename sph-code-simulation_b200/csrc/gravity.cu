@@ -34,7 +34,11 @@
 // test (Tuckerman's) and the IEEE operations taken only when the test could
 // not prove it (bit-identical on all 8.78 M particles; 126.0 ms with the
 // monopoles alone, 156.8 ms with the leaf pairs too, against 112.0 ms: the
-// proof costs more issue slots than the IEEE sequences it replaces).  Kept: the squared edge of
+// proof costs more issue slots than the IEEE sequences it replaces); an
+// accepted node's monopole terms formed one iteration later, beside the next
+// node's opening test (bit-identical; 134.1 ms under a branch, 141.7 ms
+// unconditional with selects: 103 registers against 92, fewer warps in
+// flight).  Kept: the squared edge of
 // each level from a table in shared memory instead of an ldexp per node, and
 // the next node's records loaded as soon as the opening test has chosen it
 // (116.0 -> 114.9 ms together; capped at 6 resident blocks the prefetching
