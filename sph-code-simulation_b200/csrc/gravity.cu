@@ -53,7 +53,10 @@ namespace sphgpu {
 
 namespace {
 
-constexpr int GBLK = 32;  // one warp per block: 113.5 -> 112.0 ms against 128 (256: 130.5 ms)
+// one warp per block: 113.5 -> 112.0 ms against 128 (256: 130.5 ms).  The walk
+// takes 92 registers (21 resident warps per SM); capped for 24 / 28 warps it
+// spills and takes 129.0 / 172.5 ms.
+constexpr int GBLK = 32;
 
 // subset != null: only the listed particles (the mixed form's FP64
 // re-evaluation); those launches add to no work counter.
