@@ -295,8 +295,9 @@ int sphgpu_integrate(sphgpu_ctx* ctx);
    writes it.  Fields that are final early in the step (positions and mass
    after the tree build, the PreInteraction outputs after it) are copied to
    the host while the rest of the step runs, on a second stream, and the
-   alpha, Balsara and grad-h inputs (first read by PreInteraction) are copied
-   up while the step's first modules run; the call returns when every copy
+   alpha, Balsara, grad-h, density and pressure inputs (first read by
+   PreInteraction) are copied up while the step's first modules run; the
+   call returns when every copy
    is done.  Either table may hold NULL entries. */
 int sphgpu_integrate_host(sphgpu_ctx* ctx, const double* const* in_fields, double* const* out_fields);
 /* Solver::compute_total_energies (src/solver.cpp:1149-1175), plus total

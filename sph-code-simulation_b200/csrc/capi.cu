@@ -392,10 +392,10 @@ __global__ void k_get_all(DevState S, FieldSlots F, int n)
     }
 }
 
-// sphgpu_integrate_host: the alpha / Balsara / grad-h fields uploaded beside
-// the tree build, written once the particles are in tree order (slot by the
-// caller index each particle carries)
-__global__ void k_put_visc(DevState S, FieldSlots F, int n)
+// sphgpu_integrate_host: the alpha / Balsara / grad-h and density / pressure
+// fields uploaded beside the tree build, written once the particles are in
+// tree order (slot by the caller index each particle carries)
+__global__ void k_put_late(DevState S, FieldSlots F, int n)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if(p >= n) return;
@@ -405,6 +405,12 @@ __global__ void k_put_visc(DevState S, FieldSlots F, int n)
     if(F.p[SPHGPU_F_BALSARA]) v.y = F.p[SPHGPU_F_BALSARA][k];
     if(F.p[SPHGPU_F_GRADH]) v.z = F.p[SPHGPU_F_GRADH][k];
     S.visc[p] = v;
+    if(F.p[SPHGPU_F_DENS] || F.p[SPHGPU_F_PRES]) {
+        double4 t = S.thermo[p];
+        if(F.p[SPHGPU_F_DENS]) t.x = F.p[SPHGPU_F_DENS][k];
+        if(F.p[SPHGPU_F_PRES]) t.y = F.p[SPHGPU_F_PRES][k];
+        S.thermo[p] = t;
+    }
 }
 
 // Staging for `slots` fields of n doubles, grown on demand and kept.
@@ -886,7 +892,7 @@ int integrate_host_step(sphgpu_ctx* c, double* const* out, double* dt_h, const F
     if(has_late) {
         // the fields PreInteraction reads first arrived beside the tree build
         SPHGPU_CUDA(c, cudaStreamWaitEvent(c->stream, c->copy_ev[2], 0));
-        k_put_visc<<<grid_for(c->n, 256), 256, 0, c->stream>>>(c->s, late, c->n);
+        k_put_late<<<grid_for(c->n, 256), 256, 0, c->stream>>>(c->s, late, c->n);
         SPHGPU_LAUNCH_CHECK(c, "integrate_host late fields");
     }
     if((rc = download_group_after(c, out, 0, &slot, c->copy_ev[0])) < 0) return rc;
@@ -916,10 +922,12 @@ int sphgpu_integrate_host(sphgpu_ctx* c, const double* const* in_fields, double*
     }
     int rc = ensure_stage(c, std::max(in_slots, out_slots));
     if(rc) return rc;
-    // alpha, Balsara and grad-h are first read by PreInteraction: they go up
-    // on the copy stream while the step's first modules run (srgsph contexts
+    // alpha, Balsara, grad-h, density and pressure are first read by
+    // PreInteraction (its gather walk guesses h from the density; TimeStep
+    // does not read them and predict carries them unchanged): they go up on
+    // the copy stream while the step's first modules run (srgsph contexts
     // take every field before the step)
-    const int late_f[3] = {SPHGPU_F_ALPHA, SPHGPU_F_BALSARA, SPHGPU_F_GRADH};
+    const int late_f[5] = {SPHGPU_F_ALPHA, SPHGPU_F_BALSARA, SPHGPU_F_GRADH, SPHGPU_F_DENS, SPHGPU_F_PRES};
     const bool split = c->prm.sph_type != SPHGPU_SRGSPH;
     const double* early[SPHGPU_NFIELDS];
     for(int f = 0; f < SPHGPU_NFIELDS; ++f) early[f] = in_fields[f];
