@@ -133,9 +133,13 @@ typedef struct sphgpu_params {
      * times the gather radius and later steps reuse them, moved to each new
      * tree's particle order, while every particle's gather sphere stays
      * inside its list's sphere (displacements are tracked); the consumers
-     * take exactly the reference's list members from them.  Two builds in
-     * a row that are never reused pause the skin for 32 steps.  0 = a fresh
-     * exact walk every step.  (0.02)                                      */
+     * take exactly the reference's list members from them.  The skin
+     * widens (2x, up to 5 x gather_skin) after two builds in a row that
+     * served fewer than two steps, when the motion measured at the failed
+     * check shows the wider lists would serve two; lists that serve eight
+     * steps or more narrow it again.  Two builds in a row that are never
+     * reused and do not widen it pause the skin for 32 steps of exact
+     * walks.  0 = a fresh exact walk every step.  (0.02)                  */
     double  gather_skin;
 } sphgpu_params;
 

@@ -181,6 +181,10 @@ void free_all(sphgpu_ctx* c)
     c->skin_map_pending = false;
     c->skin_built = false;
     c->skin_since_build = c->skin_idle = c->skin_off = 0;
+    c->skin_scale = 1.0;
+    c->skin_short = 0;
+    c->skin_factor = 1.0;
+    c->skin_need = -1.0;
 }
 
 template <typename T>

@@ -71,6 +71,10 @@ struct sphgpu_ctx {
     int skin_since_build = 0;        // reuses of the current skin lists
     int skin_idle = 0;               // consecutive builds that were never reused
     int skin_off = 0;                // steps left of exact walks (skin paused)
+    double skin_scale = 1.0;         // the next build's skin, in units of gather_skin
+    int skin_short = 0;              // consecutive builds whose lists served < 2 steps
+    double skin_factor = 1.0;        // 1 + the skin of the current lists
+    double skin_need = -1.0;         // skin the last failed check needed (< 0: none)
     // pair lists built from the gather lists (flist.cu)
     int* d_tcount = nullptr;         // entries appended to each row from the back
     int* d_flist_flags = nullptr;    // {incomplete, longest list, over neighborNumber * 1000}

@@ -705,18 +705,48 @@ __global__ void k_skin_guess(DevParams P, DevState S, int n, double ratio, const
     if((threadIdx.x & 31) == 0 && d > 0.0) atomic_max_pos(dmax, d);
 }
 
+__device__ __forceinline__ double skin_need_radius(const DevParams& P, const DevState& S, int i,
+                                                   const double4* __restrict__ xb, double dmax, double delta)
+{
+    const double4 p = S.pos[i];
+    const double4 b = xb[i];
+    const Vec3d v = rij(P, p.x, p.y, p.z, b.x, b.y, b.z);
+    const double d = sqrt(v.x * v.x + v.y * v.y + v.z * v.z) * (1.0 + 1e-12);
+    return (S.vel[i].w + d + dmax) * (1.0 + 1e-12) + 2.0 * delta;
+}
+
 __global__ void k_skin_check(DevParams P, DevState S, int n, const double* __restrict__ fr,
                              const double4* __restrict__ xb, const double* __restrict__ dmax, double delta,
                              int* __restrict__ bad)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= n) return;
-    const double4 p = S.pos[i];
-    const double4 b = xb[i];
-    const Vec3d v = rij(P, p.x, p.y, p.z, b.x, b.y, b.z);
-    const double d = sqrt(v.x * v.x + v.y * v.y + v.z * v.z) * (1.0 + 1e-12);
-    const double need = (S.vel[i].w + d + *dmax) * (1.0 + 1e-12) + 2.0 * delta;
-    if(!(need < fr[i])) *bad = 1;
+    if(!(skin_need_radius(P, S, i, xb, *dmax, delta) < fr[i])) *bad = 1;
+}
+
+// After a failed check: the largest skin any particle needed, in units of the
+// gather radius the lists were built for (fr / factor), i.e. the largest
+// need * factor / fr - 1 (one atomic per block of SKB).
+constexpr int SKB = 256;
+__global__ void __launch_bounds__(SKB) k_skin_need(DevParams P, DevState S, int n, const double* __restrict__ fr,
+                                                   const double4* __restrict__ xb, const double* __restrict__ dmax,
+                                                   double delta, double factor,
+                                                   unsigned long long* __restrict__ need_max)
+{
+    __shared__ double sm[SKB / 32];
+    const int i = blockIdx.x * SKB + threadIdx.x;
+    double q = 0.0;
+    if(i < n) {
+        q = skin_need_radius(P, S, i, xb, *dmax, delta) * factor / fr[i] - 1.0;
+        if(!(q >= 0.0)) q = 0.0;
+    }
+    q = warp_max_pos(q);
+    if((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = q;
+    __syncthreads();
+    if(threadIdx.x == 0) {
+        for(int w = 1; w < SKB / 32; ++w) q = fmax(q, sm[w]);
+        if(q > 0.0) atomicMax(need_max, (unsigned long long)__double_as_longlong(q));
+    }
 }
 
 // Lists, counts, radii and build positions of the previous particle order
@@ -839,7 +869,7 @@ int skin_alloc(sphgpu_ctx* c)
         c->d_skin_new = reinterpret_cast<int*>(take(4 * n));
         c->d_skin_map = reinterpret_cast<uint32_t*>(take(4 * n));
         c->d_skin_src = reinterpret_cast<uint32_t*>(take(4 * n));
-        c->d_skin_scal = reinterpret_cast<double*>(take(16));
+        c->d_skin_scal = reinterpret_cast<double*>(take(24));
         c->skin_n = c->n;
         c->skin_valid = false;
         c->skin_map_pending = false;
@@ -901,7 +931,8 @@ int skin_upload(sphgpu_ctx* c)
 
 int gather_lists(sphgpu_ctx* c, double ratio)
 {
-    constexpr int SKIN_PAUSE = 32;  // steps of exact walks after two unused builds
+    constexpr int SKIN_PAUSE = 32;     // steps of exact walks after two unused builds
+    constexpr double SKIN_GROW = 5.0;  // the widest skin, in units of gather_skin
     if(!c->have_tree) return fail(c, SPHGPU_ERR_STATE, "neighbour search before tree make");
     const double skin = c->prm.gather_skin;
     if(!(skin > 0.0) || c->walk_mode != 0) return gather_walk(c, true, ratio);
@@ -916,9 +947,11 @@ int gather_lists(sphgpu_ctx* c, double ratio)
     if(!(c->skin_delta_now < 1e299)) return gather_walk(c, true, ratio);
     if(c->skin_valid) {
         stage_begin(c, SPHGPU_T_GATHER_WALK);
+        // {largest displacement, failed-check flag, largest skin needed}
         double* dmax = c->d_skin_scal;
         int* bad = reinterpret_cast<int*>(c->d_skin_scal + 1);
-        SPHGPU_CUDA(c, cudaMemsetAsync(c->d_skin_scal, 0, 16, st));
+        auto* need = reinterpret_cast<unsigned long long*>(c->d_skin_scal + 2);
+        SPHGPU_CUDA(c, cudaMemsetAsync(c->d_skin_scal, 0, 24, st));
         k_skin_guess<<<grid_for(n, 256), 256, 0, st>>>(c->dp, c->s, n, ratio, c->d_skin_x, dmax);
         k_skin_check<<<grid_for(n, 256), 256, 0, st>>>(c->dp, c->s, n, c->d_skin_r, c->d_skin_x, dmax,
                                                         c->skin_delta_now, bad);
@@ -926,17 +959,44 @@ int gather_lists(sphgpu_ctx* c, double ratio)
         int hbad = 1;
         SPHGPU_CUDA(c, cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
         SPHGPU_CUDA(c, cudaStreamSynchronize(st));
-        stage_end(c, SPHGPU_T_GATHER_WALK, 2);
+        if(hbad) {
+            k_skin_need<<<grid_for(n, SKB), SKB, 0, st>>>(c->dp, c->s, n, c->d_skin_r, c->d_skin_x, dmax,
+                                                          c->skin_delta_now, c->skin_factor, need);
+            SPHGPU_LAUNCH_CHECK(c, "skin need");
+            double hneed = -1.0;
+            SPHGPU_CUDA(c, cudaMemcpyAsync(&hneed, need, sizeof hneed, cudaMemcpyDeviceToHost, st));
+            SPHGPU_CUDA(c, cudaStreamSynchronize(st));
+            c->skin_need = hneed;
+        }
+        stage_end(c, SPHGPU_T_GATHER_WALK, hbad ? 3 : 2);
         if(!hbad) {
             ++c->skin_reuses;
             ++c->skin_since_build;
             return SPHGPU_OK;
         }
     }
-    // a build whose lists were never reused was wasted work (the wider walk,
-    // the longer lists); after two in a row the skin pauses
-    c->skin_idle = c->skin_built && c->skin_since_build == 0 ? c->skin_idle + 1 : 0;
+    // two builds in a row whose lists served fewer than two steps: the next
+    // build takes twice the skin (up to SKIN_GROW times gather_skin), when
+    // the failed check shows that a skin within that bound would have served
+    // two steps of the same motion; lists that served eight or more: half
+    // (down to gather_skin).  A build whose lists were never reused and that
+    // does not widen the skin was wasted work (the wider walk, the longer
+    // lists); after two in a row the skin pauses
+    if(c->skin_built) {
+        const int used = c->skin_since_build;
+        c->skin_short = used < 2 ? c->skin_short + 1 : 0;
+        const double want = c->skin_need >= 0.0 ? 2.0 * c->skin_need / (double)(used + 1) / skin : 1e300;
+        const bool grow = c->skin_short >= 2 && c->skin_scale < SKIN_GROW && want <= SKIN_GROW;
+        if(grow)
+            c->skin_scale = std::min(2.0 * c->skin_scale, SKIN_GROW);
+        else if(used >= 8)
+            c->skin_scale = std::max(0.5 * c->skin_scale, 1.0);
+        c->skin_idle = !grow && used == 0 ? c->skin_idle + 1 : 0;
+    } else {
+        c->skin_idle = 0;
+    }
     c->skin_since_build = 0;
+    c->skin_need = -1.0;
     if(c->skin_idle >= 2) {
         c->skin_idle = 0;
         c->skin_off = SKIN_PAUSE - 1;
@@ -956,7 +1016,8 @@ int gather_lists(sphgpu_ctx* c, double ratio)
     c->skin_valid = false;
     stage_begin(c, SPHGPU_T_GATHER_WALK);
     int launches = 0;
-    rc = run_walk(c, 0, true, ratio, false, 0, &launches, SkinOut{1.0 + skin, c->d_skin_r, c->d_skin_x});
+    c->skin_factor = 1.0 + skin * c->skin_scale;
+    rc = run_walk(c, 0, true, ratio, false, 0, &launches, SkinOut{c->skin_factor, c->d_skin_r, c->d_skin_x});
     stage_end(c, SPHGPU_T_GATHER_WALK, launches);
     if(rc == SPHGPU_ERR_NEIGHBOR_OVERFLOW) return gather_walk(c, true, ratio);  // decided on the exact lists
     if(rc < 0) return rc;

@@ -47,8 +47,10 @@ def test_skin_lists_match_exact_walk(gpu, case, skin):
     if skin >= 0.05:
         assert c1["skin_reuses"] >= 1, c1     # the reuse path ran
     else:
-        # lists never reused: two unused builds pause the skin (exact walks)
-        assert c1["skin_builds"] <= 3, c1
+        # a skin too thin to be reused widens (2x, then 4x, after two builds
+        # in a row that served fewer than two steps); two unused builds at the
+        # widest pause it (exact walks)
+        assert c1["skin_builds"] <= 5, c1
     assert c1["skin_builds"] + c1["skin_reuses"] <= 6
     for s, (a, b) in enumerate(zip(out, ref)):
         np.testing.assert_array_equal(a["neighbor"], b["neighbor"], err_msg=f"step {s + 1}")
