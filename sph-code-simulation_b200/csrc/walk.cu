@@ -986,7 +986,15 @@ int gather_lists(sphgpu_ctx* c, double ratio)
         const int used = c->skin_since_build;
         c->skin_short = used < 2 ? c->skin_short + 1 : 0;
         const double want = c->skin_need >= 0.0 ? 2.0 * c->skin_need / (double)(used + 1) / skin : 1e300;
-        const bool grow = c->skin_short >= 2 && c->skin_scale < SKIN_GROW && want <= SKIN_GROW;
+        bool grow = c->skin_short >= 2 && c->skin_scale < SKIN_GROW && want <= SKIN_GROW;
+        if(grow) {
+            // wider lists need longer rows in both list buffers: widen only
+            // with twice the present buffers free (a second buffer that no
+            // longer fits would end the skin lists for good)
+            size_t free_b = 0, total_b = 0;
+            const size_t lists_b = 2 * sizeof(int) * (size_t)n * (size_t)c->gcap;
+            if(cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || free_b < 2 * lists_b) grow = false;
+        }
         if(grow)
             c->skin_scale = std::min(2.0 * c->skin_scale, SKIN_GROW);
         else if(used >= 8)
